@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark: LLG RK4 steps/s at 256x256x3 on one B200 (per GPU: replicas).
+
+One "step" is one classical RK4 step of the resident FP64 state: four demag
+field evaluations (divergence -> potential -> fused field/LLG/RK4 stage) plus
+the time advance, captured as one CUDA graph.  Workload: a 256x256x3 grid of
+5 nm cells holding an 8x8 lattice of permalloy discs (radius 12 cells, pitch
+32) in the middle layer, a random in-plane direction per dot, and an external
+field ramped along x from -50 to +50 mT over 10 ns; dt = 1e-13 s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--solver fmm|direct]
+    python bench.py --impl reference ...   # the reference's own CPU path
+
+Under torchrun each rank advances its own replica (seed 2010 + rank) with no
+data-path collective; the timed region is bracketed by barriers and the max
+over ranks is reported.  Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mms-gpu_b200"))
+
+METRIC = "LLG RK4 steps/s, 256x256x3: FMM vs surrogate demag at ≤1e-3 rel err vs FP64"
+WORKLOAD = "llg_rk4_disc_lattice_256x256x3"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--solver", choices=["fmm", "direct"], default=os.environ.get("MMS_BENCH_SOLVER", "fmm"))
+    ap.add_argument("--order", type=int, default=8, help="FMM expansion order P")
+    ap.add_argument("--leaf", type=int, default=0, help="FMM leaf side in cells (0 = autotuned)")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--dt", type=float, default=1e-13)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(size, seed):
+    from mmsb200 import geometry
+    X = Y = size
+    Z = 3
+    pitch = 32 * size // 256
+    r = 12 * size // 256
+    mask, M = geometry.per_dot_random_inplane(X, Y, Z, r, pitch, seed)
+    hext_t = [0.0, 1e-8]
+    hext_b = [[-0.05, 0.0, 0.0], [0.05, 0.0, 0.0]]
+    return (X, Y, Z), (5e-9, 5e-9, 5e-9), mask, M, hext_t, hext_b
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """samples SM clocks and throttle reasons with nvidia-smi during the timed region"""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [v.strip() for v in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------- helpers
+def dist_init():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def profile_traffic(kernel_key):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/<kernel_key>.md, line 'traffic_bytes_per_launch: N')"""
+    path = os.path.join(ROOT, "profiles", kernel_key + ".md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def cpu_baseline(dims, d, M, hext, steps_cap_s=60.0):
+    """The reference's own CPU direct path (oracle/_ref, built from its
+    sources), one Hfield per sample, all host threads.  steps/s = 1/(4 t_H):
+    an RK4 step of the reference is four Hfield calls (ode_functions.cpp:109,
+    121, 133, 267) and the potential is >90 % of each."""
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    if not ref.available():
+        return None
+    t, th = ref.time_hfield(M.astype(np.float32), dims, d, use_fmm=False, reps=1, threads=threads)
+    return {"value": 1.0 / (4.0 * t), "unit": "steps/s", "cores": th, "kind": "reference",
+            "sample": f"1 reference Hfield (CPU direct, OpenMP) at {dims[0]}x{dims[1]}x{dims[2]}: "
+                      f"{t:.3f} s; steps/s = 1/(4 x that)", "seconds_per_hfield": t}
+
+
+# ---------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    dims, d, mask, M, _, _ = workload(args.size, 2010)
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/mmsref_harness not built "
+                          "(the reference tree was absent when building)"}))
+        return 0
+    threads = os.cpu_count() or 1
+    Mf = M.astype(np.float32)
+    times = []
+    for _ in range(min(args.warmup, 1)):
+        ref.time_hfield(Mf, dims, d, reps=1, threads=threads)
+    t_start = time.time()
+    for _ in range(args.steps):
+        s, th = ref.time_hfield(Mf, dims, d, reps=1, threads=threads)
+        times.append(s)
+        if time.time() - t_start > 150:  # keep the whole run within a few minutes
+            break
+    t_h = float(np.mean(times))
+    v = 1.0 / (4.0 * t_h)
+    N = dims[0] * dims[1] * dims[2]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus,
+            "steps": len(times), "warmup": min(args.warmup, 1), "ms_per_step": 4 * t_h * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": list(dims), "cells": N, "cell_nm": 5,
+                       "path": "reference CPU direct sum (calc_potential_exact, use_gpu=0) inside Hfield",
+                       "threads": th},
+            "cell_steps_per_s": v * N,
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": th, "kind": "reference",
+                             "sample": f"{len(times)} reference Hfield calls at {dims[0]}x{dims[1]}x{dims[2]}, "
+                                       f"mean {t_h:.3f} s; one RK4 step = 4 Hfield"},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import mmsb200
+    ws, rank, local = dist_init()
+    dims, d, mask, M, hext_t, hext_b = workload(args.size, 2010 + rank)
+    X, Y, Z = dims
+    N = X * Y * Z
+    grid = mmsb200.Grid(X, Y, Z, *d)
+    params = mmsb200.make_params(external=True, hext_t=hext_t, hext_b=hext_b)
+    kind = mmsb200.SOLVER_FMM if args.solver == "fmm" else mmsb200.SOLVER_DIRECT
+    solver = mmsb200.make_solver(kind, args.order, args.leaf)
+    stream = torch.cuda.current_stream()
+    ctx = mmsb200.Context(grid, params, solver, stream=stream.cuda_stream)
+    ctx.state_set(mask, M)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    # accuracy of the demag potential on the start state vs the exact (direct) sum
+    acc = None
+    if args.solver == "fmm":
+        Mf = torch.from_numpy(M.astype(np.float32)).cuda()
+        rho = torch.empty((Z, Y, X), dtype=torch.float32, device="cuda")
+        phi_f = torch.empty_like(rho)
+        phi_d = torch.empty_like(rho)
+        ctx.divergence_dev(Mf, rho)
+        ctx.potential_dev(rho, phi_f)
+        with mmsb200.Context(grid, params, mmsb200.make_solver(mmsb200.SOLVER_DIRECT),
+                             stream=stream.cuda_stream) as dctx:
+            dctx.potential_dev(rho, phi_d)
+            dctx.sync()
+        acc = float((phi_f.double() - phi_d.double()).norm() / phi_d.double().norm())
+        del Mf, rho, phi_f, phi_d
+
+    # warm-up (also captures the step graph)
+    ctx.run_fixed(args.dt, max(args.warmup, 3), use_graph=True)
+    ctx.sync()
+
+    # timed region: K steps, L2 flushed between steps, per-step device events
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = ctx.kernel_launches
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        ctx.run_fixed(args.dt, 1, use_graph=True)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.kernel_launches - launches0
+    barrier(ws)
+    clk = clocks.stop()
+    ms_steps = [a.elapsed_time(b) for a, b in ev]
+    ms_total = max_over_ranks(ws, float(np.sum(ms_steps)))
+    ms_per_step = ms_total / args.steps
+    value = ws * args.steps / (ms_total * 1e-3)
+
+    # dominant kernel time inside one step, measured live with events around
+    # one potential evaluation on the same stream (the stage kernels and the
+    # divergence are the rest of the step)
+    rho_t = torch.empty((Z, Y, X), dtype=torch.float32, device="cuda")
+    phi_t = torch.empty_like(rho_t)
+    Mf = torch.from_numpy(ctx.state_get()[0].astype(np.float32)).cuda()
+    ctx.divergence_dev(Mf, rho_t)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    pot_ms = []
+    for _ in range(reps):
+        flush.fill_(1.0)
+        e0.record(stream)
+        ctx.potential_dev(rho_t, phi_t)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        pot_ms.append(e0.elapsed_time(e1))
+    pot_ms = float(np.median(pot_ms))
+    fma_peak = mmsb200.fma_tflops()
+    if args.solver == "direct":
+        pairs = float(N) * float(N) - N
+        roof = {"kernel": "k_direct (potential, exact direct sum)", "bound": "fp32",
+                "achieved": 2 * pairs / (pot_ms * 1e-3) / 1e12, "peak": fma_peak, "unit": "TFLOP/s",
+                "peak_source": "measured FP32 FMA microbenchmark (mms_diag_fma_tflops)",
+                "algorithmic": "2 flops (one FMA) per target-source pair, N^2 - N pairs"}
+        roof["frac"] = roof["achieved"] / roof["peak"]
+        roof["traffic"] = profile_traffic("k_direct_256x256x3")
+    else:
+        info = fmm_roofline(ctx, pot_ms, fma_peak)
+        roof = info
+    roof["potential_ms"] = pot_ms
+    roof["potential_share_of_step"] = 4 * pot_ms / ms_per_step
+
+    # e2e through the public API with host buffers: H2D of the state, one step,
+    # D2H of the state, every step
+    e2e = None
+    if not args.no_e2e:
+        host_M = torch.from_numpy(ctx.state_get()[0]).pin_memory()
+        host_mat = torch.from_numpy(mask.astype(np.uint8)).pin_memory()
+        dev_M = torch.empty(host_M.shape, dtype=torch.float64, device="cuda")
+        dev_mat = torch.empty(host_mat.shape, dtype=torch.uint8, device="cuda")
+        out_M = torch.empty_like(host_M).pin_memory()
+        t = 0.0
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            ev2[k][0].record(stream)
+            dev_M.copy_(host_M, non_blocking=True)
+            dev_mat.copy_(host_mat, non_blocking=True)
+            ctx.state_set_dev(dev_mat, dev_M, t)
+            ctx.run_fixed(args.dt, 1, use_graph=True)
+            ctx.state_get_dev(dev_M)
+            out_M.copy_(dev_M, non_blocking=True)
+            ev2[k][1].record(stream)
+            t += args.dt
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(ws, float(sum(a.elapsed_time(b) for a, b in ev2)))
+        e2e = {"value": ws * args.steps / (e2e_ms * 1e-3), "unit": "steps/s",
+               "h2d_bytes_per_step": int(host_M.numel() * 8 + host_mat.numel()),
+               "d2h_bytes_per_step": int(out_M.numel() * 8),
+               "path": "mms_state_set_dev + mms_run_fixed(1 step) + mms_state_get_dev, pinned host copies"}
+
+    base = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            base = cpu_baseline(dims, d, M, (hext_t, hext_b))
+        except Exception as e:  # the baseline is reported, never required
+            base = {"value": None, "error": str(e)[:200]}
+
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    cfg = {"workload": WORKLOAD, "grid": [X, Y, Z], "cells": N, "cell_nm": 5, "solver": args.solver,
+           "dt_s": args.dt, "state": "fp64", "fields": "fp32",
+           "geometry": "8x8 lattice of discs r=12 pitch 32 (middle layer), random in-plane M per dot",
+           "external": "B_x ramp -50..+50 mT over 10 ns", "l2": f"flushed between timed steps "
+           f"({L2_FLUSH_BYTES >> 20} MB write, outside the timed events)", "graph": "one CUDA graph per RK4 step",
+           "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
+    if args.solver == "fmm":
+        cfg.update({"P": args.order, "leaf": args.leaf or "auto"})
+    line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": cfg,
+            "cell_steps_per_s": value * N, "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
+            "e2e": e2e, "cpu_baseline": base}
+    if acc is not None:
+        line["accuracy"] = {"demag_phi_rel_l2_vs_direct": acc,
+                            "note": "direct = exact FP32 table + compensated sum, itself <= 2e-6 from FP64"}
+    print(json.dumps(line))
+    return 0
+
+
+def fmm_roofline(ctx, pot_ms, fma_peak):
+    """FMM roofline: the whole potential evaluation against the FP32 pipe (its
+    dominant stages, P2P and M2L on the SIMT path, are FP32-bound)"""
+    import mmsb200
+    st = mmsb200.fmm_stats(ctx)
+    roof = {"kernel": "FMM potential (P2M..L2P + P2P)", "bound": "fp32", "peak": fma_peak, "unit": "TFLOP/s",
+            "peak_source": "measured FP32 FMA microbenchmark (mms_diag_fma_tflops)"}
+    roof["achieved"] = st["flops"] / (pot_ms * 1e-3) / 1e12
+    roof["frac"] = roof["achieved"] / fma_peak
+    roof["algorithmic"] = st
+    roof["traffic"] = profile_traffic("fmm_256x256x3")
+    return roof
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

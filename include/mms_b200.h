@@ -1,0 +1,180 @@
+/*
+ * mms_b200 — B200-native (sm_100a) demag / LLG hot path of mms-gpu.
+ *
+ * Plain C ABI: plain pointers and sizes, no C++ or torch types.  A context
+ * owns everything sized by the grid (device buffers, the FMM plan, the kernel
+ * table of the direct sum, CUDA graphs); the caller owns its input/output
+ * arrays.  Every entry point returns an mms_status; on failure
+ * mms_last_error() gives a message (thread-local).  Nothing here calls exit().
+ *
+ * Conventions shared with the reference (akhan3/mms-gpu):
+ *   cell index i = z*ydim*xdim + y*xdim + x          (vector_functions.cpp:20-26)
+ *   vector fields at the boundary are FP32 AoS {x,y,z} triples (Vector3.hpp:10-12)
+ *   potential phi_i = sum_{j != i} rho_j dV / |r_i - r_j|, WITHOUT 1/(4 pi)
+ *                                                   (fmm_calc.cu:412-461)
+ *   H_demag = (1/(4 pi)) * central-difference grad(phi) (ode_functions.cpp:51)
+ *
+ * Entry points and the reference interface each one replaces:
+ *   mms_potential_dev / mms_potential_host
+ *        <- calc_potential_exact   helper_functions.hpp:31-35 (solver DIRECT)
+ *        <- calc_potential_exact_gpu helper_functions.hpp:37-40
+ *        <- fmm_calc               helper_functions.hpp:24-29 (solver FMM)
+ *   mms_hfield_dev / mms_hfield_host
+ *        <- Hfield                 ode_functions.hpp:8-15
+ *   mms_divergence_dev, mms_gradient_dev, mms_exchange_dev
+ *        <- divergence_3d / gradient_3d / add_exchange_field
+ *                                  vector_functions.hpp:9-25
+ *   mms_state_*, mms_rk4_step, mms_run_fixed
+ *        <- rk4_step               ode_functions.cpp:76-87 (no header upstream)
+ *   mms_march                      <- time_marching ode_functions.hpp:17-24
+ * The C++ shim with the reference's exact signatures is include/mms_ref_api.hpp.
+ */
+#ifndef MMS_B200_H
+#define MMS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MMS_ABI_VERSION 1
+
+typedef enum {
+    MMS_OK = 0,
+    MMS_ERR_ARG = 1,         /* bad argument / unsupported size               */
+    MMS_ERR_CUDA = 2,        /* a CUDA runtime call failed                    */
+    MMS_ERR_NOMEM = 3,       /* device or host allocation failed              */
+    MMS_ERR_NUMERIC = 4,     /* NaN/Inf detected in a field or the state      */
+    MMS_ERR_NOT_READY = 5,   /* state not initialised                         */
+    MMS_ERR_REJECTED = 6     /* step controller gave up (too many rejections) */
+} mms_status;
+
+typedef enum {
+    MMS_SOLVER_DIRECT = 0,   /* exact O(N^2) sum, FP32 tiles, compensated      */
+    MMS_SOLVER_FMM = 1       /* spherical-harmonic FMM, exact near field       */
+} mms_solver_kind;
+
+typedef struct {
+    int xdim, ydim, zdim;    /* cells                                          */
+    double dx, dy, dz;       /* cell size (m)                                  */
+} mms_grid;
+
+typedef struct {
+    double Ms;               /* saturation magnetisation (A/m)                 */
+    double Aexch;            /* exchange constant (J/m)                        */
+    double alpha;            /* damping                                        */
+    double gamma;            /* gyromagnetic ratio (m/(A s))                   */
+    double mu0;              /* vacuum permeability                            */
+    int demag, exchange, external;
+    /* external B(t) (tesla) as a clamped piecewise-linear table; H_ext = B/mu0.
+     * n_hext == 0 with external != 0 selects the reference's built-in ramp
+     * B_x = 0.3 T -> 0 over 1 ns (ode_functions.cpp:61).  Copied at set time. */
+    int n_hext;
+    const double *hext_t;    /* n_hext times (s), increasing                  */
+    const double *hext_b;    /* n_hext x 3 (T)                                */
+    /* 1: all RK4 stages evaluate H_ext at the step start t and the post-step
+     * field at the old t, as the reference does (ode_functions.cpp:109-133,
+     * :267); 0: stage times t + c_s dt. */
+    int ref_stage_time;
+} mms_params;
+
+typedef struct {
+    int kind;                /* mms_solver_kind                                */
+    int fmm_order;           /* expansion order P (FMM), 1..12                 */
+    int fmm_leaf;            /* leaf box side in cells (FMM), 2..16, or 0=auto */
+    int reserved[5];
+} mms_solver;
+
+typedef struct mms_ctx mms_ctx;
+
+/* library / context ---------------------------------------------------------- */
+int mms_abi_version(void);
+const char *mms_last_error(void);
+/* Creates a context on the CURRENT CUDA device.  Allocates every device buffer
+ * the grid needs; no later call allocates device memory (except mms_march's
+ * host logs).  stream: a cudaStream_t (as void*), or NULL for a private one. */
+int mms_ctx_create(const mms_grid *grid, const mms_params *params, const mms_solver *solver,
+                   void *stream, mms_ctx **out);
+int mms_ctx_destroy(mms_ctx *ctx);
+int mms_ctx_set_params(mms_ctx *ctx, const mms_params *params);
+int mms_ctx_set_solver(mms_ctx *ctx, const mms_solver *solver);
+int mms_ctx_sync(mms_ctx *ctx);
+/* number of kernels this library launched through ctx so far */
+int64_t mms_ctx_kernel_launches(const mms_ctx *ctx);
+/* device bytes held by ctx */
+size_t mms_ctx_device_bytes(const mms_ctx *ctx);
+
+/* stateless field operators (device pointers, asynchronous on ctx's stream) - */
+/* rho = div M (vector_functions.cpp:8-28).  M: N x 3 FP32 AoS, rho: N FP32 */
+int mms_divergence_dev(mms_ctx *ctx, const float *M, float *rho);
+/* phi from rho with ctx's solver (fmm_calc.cu:295-461). N FP32 each */
+int mms_potential_dev(mms_ctx *ctx, const float *rho, float *phi);
+/* H = c * grad(phi) (vector_functions.cpp:31-54).  H: N x 3 FP32 AoS, overwritten */
+int mms_gradient_dev(mms_ctx *ctx, const float *phi, double c, float *H);
+/* H += exchange field of M (vector_functions.cpp:57-103) */
+int mms_exchange_dev(mms_ctx *ctx, const float *M, float *H);
+/* full effective field at time t (ode_functions.cpp:21-70).  charge/potential
+ * may be NULL (then ctx scratch is used) or N-float device outputs. */
+int mms_hfield_dev(mms_ctx *ctx, const float *M, float *H, float *charge, float *potential, double t);
+
+/* same, HOST pointers: copies in, computes, copies out, synchronises */
+int mms_potential_host(mms_ctx *ctx, const float *rho, float *phi);
+int mms_hfield_host(mms_ctx *ctx, const float *M, float *H, float *charge, float *potential, double t);
+
+/* resident FP64 state and RK4 (ode_functions.cpp:76-148) ---------------------- */
+/* material: N bytes (non-zero = magnetic), M: N x 3 FP64 AoS; host pointers.
+ * M is taken as zero at empty cells. */
+int mms_state_set(mms_ctx *ctx, const uint8_t *material, const double *M, double t);
+int mms_state_get(mms_ctx *ctx, double *M, double *t);
+/* same with device pointers (material u8, M FP64 AoS) */
+int mms_state_set_dev(mms_ctx *ctx, const uint8_t *material, const double *M, double t);
+int mms_state_get_dev(mms_ctx *ctx, double *M);
+/* nsteps classical RK4 steps of size dt, 4 field evaluations per step.  With
+ * use_graph != 0 one step is captured once as a CUDA graph and replayed. */
+int mms_run_fixed(mms_ctx *ctx, double dt, int nsteps, int use_graph);
+/* energy (eV) and max |M x H|/Ms^2 of the current state, as time_marching logs
+ * them (ode_functions.cpp:234-240, :268-278); also <M>/Ms and <|M|>/Ms */
+int mms_state_stats(mms_ctx *ctx, double *E_eV, double *torque, double Mavg[3], double *Mmag_avg);
+
+/* adaptive RK4 --------------------------------------------------------------- */
+typedef struct {
+    int mode;                /* 0: reference energy/torque controller
+                                   (ode_functions.cpp:226-341);
+                                1: RK4 step doubling, FP64 error estimate, rtol */
+    double rtol;             /* mode 1: max |M_full - M_half2| / Ms per step  */
+    double dt_min, dt_max;   /* mode 1 clamps (s)                             */
+    double torque_stop;      /* stop when max torque < this (reference 1e-3)  */
+    int max_rejects;         /* consecutive rejections before giving up (50)  */
+    int reserved[3];
+} mms_controller;
+
+typedef struct {             /* one record per accepted step, the 9 columns of
+                                dynamics.dat (ode_functions.cpp:330-333)       */
+    int tindex;
+    double t, dt, E_eV, Mx, My, Mz, Mmag, torque;
+} mms_record;
+
+/* Called after every accepted step (rejected = 0) and every rejected attempt
+ * (rejected = 1; rec->dt is then the reduced step).  The state may be read
+ * with mms_state_get inside the callback.  A non-zero return stops marching. */
+typedef int (*mms_march_cb)(void *user, int rejected, const mms_record *rec);
+
+/* March until t > finaltime, the torque stop, or controller failure.
+ * records: caller array of max_records (may be NULL); *n_records receives the
+ * number of accepted steps.  cb may be NULL.  Returns MMS_ERR_REJECTED after
+ * max_rejects consecutive rejections. */
+int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double dt0,
+              mms_record *records, int max_records, int *n_records, mms_march_cb cb, void *user);
+
+/* diagnostics ---------------------------------------------------------------- */
+/* FP32 FMA throughput of the current device in TFLOP/s (a microbenchmark of
+ * `reps` launches, one wave of 8 CTAs per SM): the roofline denominator of the
+ * FP32-pipe-bound kernels (direct sum, near field).  No reference counterpart. */
+int mms_diag_fma_tflops(int reps, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,159 @@
+// Internal declarations shared by the mms_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "mms_b200.h"
+
+// ---------------------------------------------------------------------------
+// error plumbing: every failure becomes a status code and a thread-local message
+void mms_set_error(const char *fmt, ...);
+
+#define MMS_CUDA_TRY(expr)                                                                  \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess) {                                                            \
+            mms_set_error("%s:%d %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(e_)); \
+            return MMS_ERR_CUDA;                                                            \
+        }                                                                                   \
+    } while (0)
+
+#define MMS_TRY(expr)                  \
+    do {                               \
+        int s_ = (expr);               \
+        if (s_ != MMS_OK) return s_;   \
+    } while (0)
+
+// after a launch: check the launch itself (asynchronous faults surface at sync)
+#define MMS_LAUNCH_CHECK(ctx)                                                               \
+    do {                                                                                    \
+        (ctx)->launches++;                                                                  \
+        cudaError_t e_ = cudaGetLastError();                                                \
+        if (e_ != cudaSuccess) {                                                            \
+            mms_set_error("%s:%d kernel launch: %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+            return MMS_ERR_CUDA;                                                            \
+        }                                                                                   \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device-side constants of a grid / material, passed by value to kernels
+struct GridK {
+    int X, Y, Z;
+    long long N;
+    double dx, dy, dz;
+};
+
+constexpr int MMS_MAX_HEXT = 64;
+
+struct PhysK {
+    double Ms, alpha, gamma, mu0;
+    double cexch;        // 2 A / (mu0 Ms^2)
+    double cdemag;       // 1 / (4 pi)
+    int demag, exchange, external;
+    int n_hext;          // 0 + external: the reference's built-in ramp
+    int ref_stage_time;
+};
+
+// time state kept on the device so a captured step graph stays valid:
+//   [0] t      current time of the state M
+//   [1] dt     step size
+//   [2] t_k1   time at which H(M) (the k1 field) was evaluated; equals t
+//              except in reference-stage-time mode (see mms_params)
+constexpr int TIME_T = 0, TIME_DT = 1, TIME_TK1 = 2, TIME_SLOTS = 4;
+
+// statistics block: sums over material cells, finished on device
+//   [0] sum M.H  [1] max |MxH|  [2..4] sum M  [5] sum |M|  [6] count  [7] nonfinite flag
+constexpr int STAT_SLOTS = 8;
+
+struct FmmPlan;  // fmm.cu
+
+struct mms_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    mms_grid g{};
+    mms_params p{};
+    std::vector<double> hext_t, hext_b;
+    mms_solver s{};
+    long long N = 0;
+    int64_t launches = 0;
+    size_t dev_bytes = 0;
+
+    // device buffers
+    float *rho = nullptr, *phi = nullptr;       // N
+    float *vecA = nullptr, *vecB = nullptr;     // 3N FP32 AoS scratch (host API)
+    float *gtab = nullptr;                      // direct-sum kernel table X*Y*Z
+    uint8_t *mat = nullptr;                     // N
+    double *M = nullptr, *A = nullptr, *B = nullptr, *K = nullptr;  // 3N each, SoA planes
+    double *Mbak = nullptr;                     // 3N, controller backup
+    double *Mfull = nullptr;                    // 3N, step-doubling full-step result
+    float *phibak = nullptr;                    // N, controller backup
+    double *tstate = nullptr;                   // TIME_SLOTS
+    double *hext = nullptr;                     // MMS_MAX_HEXT x 4 (t, Bx, By, Bz)
+    double *stat_part = nullptr;                // per-block partial statistics
+    double *stats = nullptr;                    // STAT_SLOTS
+    int stat_blocks = 0;
+    double *h_stats = nullptr;                  // pinned host mirror of stats + time
+
+    FmmPlan *fmm = nullptr;
+
+    bool state_ready = false;
+    bool phi_valid = false;                     // phi holds the potential of M
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_kernels = 0;
+    int graph_solver_kind = -1;
+
+    GridK gk() const {
+        GridK k;
+        k.X = g.xdim; k.Y = g.ydim; k.Z = g.zdim; k.N = N;
+        k.dx = g.dx; k.dy = g.dy; k.dz = g.dz;
+        return k;
+    }
+    PhysK pk() const;
+};
+
+// ---------------------------------------------------------------------------
+// kernel entry points (host-side launchers); all asynchronous on ctx->stream
+int launch_divergence_soa(mms_ctx *ctx, const double *M, float *rho);
+int launch_divergence_aos(mms_ctx *ctx, const float *M, float *rho);
+int launch_gradient_aos(mms_ctx *ctx, const float *phi, double c, float *H);
+int launch_exchange_aos(mms_ctx *ctx, const float *M, float *H);
+int launch_hfield_aos(mms_ctx *ctx, const float *M, const float *phi, double t, float *H);
+int launch_rk4_stage(mms_ctx *ctx, int stage, const double *Mst, double *Mnext);
+int launch_advance_time(mms_ctx *ctx);
+int launch_stats(mms_ctx *ctx);
+
+int direct_build_table(mms_ctx *ctx);
+int launch_potential_direct(mms_ctx *ctx, const float *rho, float *phi);
+
+int fmm_plan_create(mms_ctx *ctx);
+void fmm_plan_destroy(mms_ctx *ctx);
+int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi);
+size_t fmm_plan_bytes(const mms_ctx *ctx);
+
+// potential with the context's solver
+int launch_potential(mms_ctx *ctx, const float *rho, float *phi);
+
+// device allocation tracked in ctx->dev_bytes
+template <class T>
+int ctx_alloc(mms_ctx *ctx, T **p, size_t count)
+{
+    size_t bytes = count * sizeof(T);
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        mms_set_error("cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        return MMS_ERR_NOMEM;
+    }
+    ctx->dev_bytes += bytes;
+    return MMS_OK;
+}
+
+static inline unsigned div_up(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
