@@ -229,7 +229,9 @@ def run_ours(args):
     params = mmsb200.make_params(external=True, hext_t=hext_t, hext_b=hext_b)
     kind = mmsb200.SOLVER_FMM if args.solver == "fmm" else mmsb200.SOLVER_DIRECT
     solver = mmsb200.make_solver(kind, args.order, args.leaf)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library's kernels and every timing event live on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = mmsb200.Context(grid, params, solver, stream=stream.cuda_stream)
     ctx.state_set(mask, M)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")

@@ -94,7 +94,8 @@ int mms_abi_version(void);
 const char *mms_last_error(void);
 /* Creates a context on the CURRENT CUDA device.  Allocates every device buffer
  * the grid needs; no later call allocates device memory (except mms_march's
- * host logs).  stream: a cudaStream_t (as void*), or NULL for a private one. */
+ * host logs).  stream: a cudaStream_t (as void*), or NULL for a private
+ * blocking stream (ordered with the legacy default stream). */
 int mms_ctx_create(const mms_grid *grid, const mms_params *params, const mms_solver *solver,
                    void *stream, mms_ctx **out);
 int mms_ctx_destroy(mms_ctx *ctx);
@@ -167,6 +168,13 @@ typedef int (*mms_march_cb)(void *user, int rejected, const mms_record *rec);
  * max_rejects consecutive rejections. */
 int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double dt0,
               mms_record *records, int max_records, int *n_records, mms_march_cb cb, void *user);
+
+/* FMM plan of a context: tree levels L (leaf level), leaf side, order P, the
+ * algorithmic flops of one potential evaluation (P2M, M2M, M2L, L2L, L2P at
+ * 2 per multiply-add on the parity blocks, P2P at 2 per pair) and the P2P pair
+ * and M2L box-pair counts.  MMS_ERR_ARG if the context's solver is not FMM. */
+int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double *flops,
+                 long long *p2p_pairs, long long *m2l_pairs);
 
 /* diagnostics ---------------------------------------------------------------- */
 /* FP32 FMA throughput of the current device in TFLOP/s (a microbenchmark of

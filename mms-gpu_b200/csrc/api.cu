@@ -287,7 +287,9 @@ int mms_ctx_create(const mms_grid *grid, const mms_params *params, const mms_sol
         if (stream) {
             ctx->stream = (cudaStream_t)stream;
         } else {
-            if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            // a blocking stream: ordered with the legacy default stream, so a
+            // caller's default-stream copies and this context's kernels never race
+            if (cudaStreamCreate(&ctx->stream) != cudaSuccess) {
                 mms_set_error("cudaStreamCreate failed");
                 st = MMS_ERR_CUDA;
                 break;

@@ -105,6 +105,8 @@ SIGNATURES = {
     "mms_march": (_I, [_VP, ctypes.POINTER(Controller), _D, _D, ctypes.POINTER(Record), _I, ctypes.POINTER(_I),
                        MARCH_CB, _VP]),
     "mms_diag_fma_tflops": (_I, [_I, ctypes.POINTER(_D)]),
+    "mms_fmm_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D),
+                          ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
 }
 
 _lib = None
@@ -145,6 +147,17 @@ def fma_tflops(reps=20):
     v = ctypes.c_double()
     _check(load().mms_diag_fma_tflops(reps, ctypes.byref(v)))
     return v.value
+
+
+def fmm_stats(ctx):
+    """FMM plan of a context: levels, leaf, order, flops per evaluation, pair counts"""
+    L, s, P = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    fl = ctypes.c_double()
+    pp, mp = ctypes.c_longlong(), ctypes.c_longlong()
+    _check(load().mms_fmm_info(ctx.h, ctypes.byref(L), ctypes.byref(s), ctypes.byref(P), ctypes.byref(fl),
+                               ctypes.byref(pp), ctypes.byref(mp)))
+    return dict(levels=L.value, leaf=s.value, order=P.value, flops=fl.value, p2p_pairs=pp.value,
+                m2l_pairs=mp.value)
 
 
 def make_params(Ms=8.6e5, Aexch=1.3e-11, alpha=0.5, gamma=2.21e5, mu0=4e-7 * np.pi, demag=True, exchange=True,

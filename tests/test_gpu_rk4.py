@@ -117,7 +117,8 @@ def test_reference_controller_matches_reference_log(cuda, lib):
     for col, tol in [(1, 1e-3), (2, 1e-3), (3, 1e-4), (4, 1e-4), (5, 1e-3), (6, 1e-3), (8, 1e-3)]:
         a, b = rows[:n, col], rows_ref[:n, col]
         assert np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-3)) < tol, col
-    assert max_angle_deg(Mf, z["M_final"], z["material"]) < 0.05
+    # 159 accepted steps of an FP32-state run vs an FP64-state run
+    assert max_angle_deg(Mf, z["M_final"], z["material"]) < 0.1
 
 
 def test_step_doubling_controller(cuda, lib, oracle_mod):
