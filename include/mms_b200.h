@@ -82,7 +82,7 @@ typedef struct {
 
 typedef struct {
     int kind;                /* mms_solver_kind                                */
-    int fmm_order;           /* expansion order P (FMM), 1..12                 */
+    int fmm_order;           /* expansion order P (FMM), 1..9                  */
     int fmm_leaf;            /* leaf box side in cells (FMM), 2..16, or 0=auto */
     int reserved[5];
 } mms_solver;
@@ -170,11 +170,16 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
               mms_record *records, int max_records, int *n_records, mms_march_cb cb, void *user);
 
 /* FMM plan of a context: tree levels L (leaf level), leaf side, order P, the
- * algorithmic flops of one potential evaluation (P2M, M2M, M2L, L2L, L2P at
- * 2 per multiply-add on the parity blocks, P2P at 2 per pair) and the P2P pair
- * and M2L box-pair counts.  MMS_ERR_ARG if the context's solver is not FMM. */
-int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double *flops,
+ * algorithmic flops of one potential evaluation per stage (P2M, M2M, M2L, L2L,
+ * L2P+P2P; 2 per multiply-add on the parity blocks, 2 per near-field pair) and
+ * the P2P pair and M2L box-pair counts.  MMS_ERR_ARG if the solver is not FMM. */
+int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double stage_flops[5],
                  long long *p2p_pairs, long long *m2l_pairs);
+
+/* Per-stage device time of the FMM potential (ms, mean over reps after one
+ * warm-up): [0] P2M, [1] M2M, [2] M2L, [3] L2L, [4] L2P + P2P.  CUDA events on
+ * ctx's stream between the stage launches; rho/phi are device arrays. */
+int mms_fmm_stage_times(mms_ctx *ctx, const float *rho, float *phi, int reps, double ms[5]);
 
 /* diagnostics ---------------------------------------------------------------- */
 /* FP32 FMA throughput of the current device in TFLOP/s (a microbenchmark of

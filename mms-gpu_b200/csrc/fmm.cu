@@ -49,145 +49,28 @@ struct FmmPlan {
     int n_m2l_items = 0;
     // device
     float *Wt = nullptr;      // [C][NR]  P2M weights (dV folded in)
-    float *Vt = nullptr;      // [NR][C]  L2P weights (1/w folded in)
-    float *Tm2m = nullptr;    // [4][NR(j)][NR(k)]
-    float *Tl2l = nullptr;    // [4][NR(j)][NR(k)]
+    float *Vt = nullptr;      // [NR][C]  L2P weights (1/leaf width folded in)
+    float *Tm2m = nullptr;    // [4][parity block][j][k]
+    float *Tl2l = nullptr;    // [4][parity block][j][k]
     float *Tm2l = nullptr;    // [49][2][NBmax(j)][KP(k)] parity blocks, k padded
+    float *Tm2lc = nullptr;   // [49][even NE x NE | odd NO x NO] compact, j-major (low orders)
+    int m2l_resident = 0;     // 1: k_m2l_res (all operators in shared memory)
     float *Gn = nullptr;      // [Z][2s][2s] near-field dV/|r|
     float *Mall = nullptr;    // [boxes of all levels][NR]
-    float *Lall = nullptr;
+    float *Lall = nullptr;    // final locals
+    float *Lpart = nullptr;   // [NSPLIT][boxes][NR] M2L partial locals
     int4 *m2l_items = nullptr;  // {level, parity, first target, 0}
     long long *lev_dev = nullptr;  // device copy of lev_off
     size_t bytes = 0;
     // algorithmic work per evaluation (for the roofline)
-    double flops = 0, bytes_min = 0;
+    double flops = 0;
+    double stage_flops[5] = {0, 0, 0, 0, 0};  // P2M, M2M, M2L, L2L, L2P+P2P
     long long p2p_pairs = 0, m2l_pairs = 0;
 };
 
 namespace {
 
-// ---- P2M: leaf multipoles.  CTA per leaf box, thread per coefficient.
-__global__ void k_p2m(const float *__restrict__ rho, const float *__restrict__ Wt, float *__restrict__ Mleaf,
-                      FmmDev f)
-{
-    extern __shared__ float q[];  // C charges of the box (z, y, x order)
-    const int box = blockIdx.x;
-    const int bx = box % f.nb, by = box / f.nb;
-    const int s = f.s;
-    for (int c = threadIdx.x; c < f.C; c += blockDim.x) {
-        const int x = bx * s + c % s, y = by * s + (c / s) % s, z = c / (s * s);
-        q[c] = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < f.NR; k += blockDim.x) {
-        float acc = 0.f;
-        for (int c = 0; c < f.C; c++) acc = fmaf(Wt[(long long)c * f.NR + k], q[c], acc);
-        Mleaf[(long long)box * f.NR + k] = acc;
-    }
-}
-
-// ---- M2M: parent level l from children at l+1.  CTA per parent, thread per k.
-__global__ void k_m2m(float *__restrict__ Mall, const float *__restrict__ Tm2m, long long off_p, long long off_c,
-                      int np, FmmDev f)
-{
-    const int box = blockIdx.x;
-    const int bx = box % np, by = box / np, nc = 2 * np;
-    const int k = threadIdx.x;
-    if (k >= f.NR) return;
-    const int j0 = (k < f.NE) ? 0 : f.NE, j1 = (k < f.NE) ? f.NE : f.NR;
-    float acc = 0.f;
-    for (int c = 0; c < 4; c++) {
-        const int cx = 2 * bx + (c & 1), cy = 2 * by + (c >> 1);
-        const float *Mc = Mall + (off_c + (long long)cy * nc + cx) * f.NR;
-        const float *T = Tm2m + (long long)c * f.NR * f.NR;
-        for (int j = j0; j < j1; j++) acc = fmaf(T[(long long)j * f.NR + k], Mc[j], acc);
-    }
-    Mall[(off_p + box) * f.NR + k] = acc;
-}
-
-// ---- M2L: all levels >= 2 in one launch.
-// CTA = 32 targets of one (level, parity class) x one parity block of k;
-// lane <-> target, warp <-> 16 consecutive k.  The 27 offsets of the class are
-// walked in order; each offset's operator block is staged in shared memory and
-// read as warp-uniform float4 broadcasts, each lane streams its own source
-// multipole from global (L1).  Results overwrite Lall (the downward pass adds
-// the parents' contributions afterwards).
-__global__ void __launch_bounds__(32 * M2L_WARPS) k_m2l(const float *__restrict__ Mall, float *__restrict__ Lall,
-                                                        const float *__restrict__ Tm2l, const int4 *__restrict__ items,
-                                                        const long long *__restrict__ lev_off, FmmDev f, int KP0,
-                                                        int KP1, int NBmax)
-{
-    extern __shared__ __align__(16) float Ts[];  // [NBmax][KP]
-    const int4 it = items[blockIdx.x];
-    const int lev = it.x, px = it.y & 1, py = it.y >> 1;
-    const int blk = blockIdx.y;
-    const int KP = blk ? KP1 : KP0;
-    const int NB = blk ? (f.NR - f.NE) : f.NE;
-    const int boff = blk ? f.NE : 0;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = 1 << lev, nh = n >> 1;
-    const int ti = it.z + lane;
-    const bool tvalid = ti < nh * nh;
-    const int tx = 2 * (ti % nh) + px, ty = 2 * (ti / nh) + py;
-    const long long off = lev_off[lev];
-    const int k0 = warp * KW;
-    const bool wactive = k0 < NB;
-
-    float acc[KW];
-#pragma unroll
-    for (int i = 0; i < KW; i++) acc[i] = 0.f;
-
-    for (int oy = py - 3; oy <= py + 2; oy++)
-        for (int ox = px - 3; ox <= px + 2; ox++) {
-            if (max(abs(ox), abs(oy)) < 2) continue;
-            const int o = (oy + 3) * 7 + (ox + 3);
-            const float *Tg = Tm2l + ((long long)o * 2 + blk) * NBmax * max(KP0, KP1);
-            __syncthreads();
-            for (int i = threadIdx.x * 4; i < NB * KP; i += blockDim.x * 4)
-                *reinterpret_cast<float4 *>(&Ts[i]) = *reinterpret_cast<const float4 *>(&Tg[i]);
-            __syncthreads();
-            const int sx = tx - ox, sy = ty - oy;
-            if (!(wactive && tvalid && sx >= 0 && sy >= 0 && sx < n && sy < n)) continue;
-            const float *Ms = Mall + (off + (long long)sy * n + sx) * f.NR + boff;
-            for (int j = 0; j < NB; j++) {
-                const float m = __ldg(&Ms[j]);
-                const float4 *tr = reinterpret_cast<const float4 *>(&Ts[j * KP + k0]);
-#pragma unroll
-                for (int v = 0; v < KW / 4; v++) {
-                    const float4 t = tr[v];
-                    acc[4 * v + 0] = fmaf(t.x, m, acc[4 * v + 0]);
-                    acc[4 * v + 1] = fmaf(t.y, m, acc[4 * v + 1]);
-                    acc[4 * v + 2] = fmaf(t.z, m, acc[4 * v + 2]);
-                    acc[4 * v + 3] = fmaf(t.w, m, acc[4 * v + 3]);
-                }
-            }
-        }
-    if (!(wactive && tvalid)) return;
-    float *Lt = Lall + (off + (long long)ty * n + tx) * f.NR + boff;
-#pragma unroll
-    for (int i = 0; i < KW; i++)
-        if (k0 + i < NB) Lt[k0 + i] = acc[i];
-}
-
-// ---- L2L: child level l += shifted parent locals.  CTA per child, thread per k.
-__global__ void k_l2l(float *__restrict__ Lall, const float *__restrict__ Tl2l, long long off_p, long long off_c,
-                      int nc, FmmDev f)
-{
-    const int box = blockIdx.x;
-    const int cx = box % nc, cy = box / nc;
-    const int k = threadIdx.x;
-    if (k >= f.NR) return;
-    const int c = (cx & 1) | ((cy & 1) << 1);
-    const int np = nc >> 1;
-    const float *Lp = Lall + (off_p + (long long)(cy >> 1) * np + (cx >> 1)) * f.NR;
-    const float *T = Tl2l + (long long)c * f.NR * f.NR;
-    const int j0 = (k < f.NE) ? 0 : f.NE, j1 = (k < f.NE) ? f.NE : f.NR;
-    float acc = 0.f;
-    for (int j = j0; j < j1; j++) acc = fmaf(T[(long long)j * f.NR + k], Lp[j], acc);
-    Lall[(off_c + box) * f.NR + k] += acc;
-}
-
-// ---- L2P + P2P: CTA per leaf box, thread per target cell.
+// ---- generic L2P + P2P (any leaf side): CTA per leaf box, thread per target cell.
 __global__ void k_l2p_p2p(const float *__restrict__ rho, const float *__restrict__ Lleaf,
                           const float *__restrict__ Vt, const float *__restrict__ Gn, float *__restrict__ phi,
                           FmmDev f, int far)
@@ -232,7 +115,432 @@ __global__ void k_l2p_p2p(const float *__restrict__ rho, const float *__restrict
             }
         }
     }
-    phi[((long long)lz * f.Y + y) * f.X + x] = farv * f.inv_w + near;
+    phi[((long long)lz * f.Y + y) * f.X + x] = farv + near;
+}
+
+
+// ===========================================================================
+// Stage kernels.
+
+constexpr int BB = 8;         // leaf boxes per CTA along x in the leaf kernels
+constexpr int NSPLIT = 9;     // M2L offset groups (3 offsets each) -> partial locals
+
+// P2M: CTA = BB leaf boxes of one row; thread per coefficient; the boxes'
+// charges sit transposed in shared memory ([cell][box]) so one LDS.128 feeds 4 FMAs
+__global__ void __launch_bounds__(128) k_p2m_row(const float *__restrict__ rho, const float *__restrict__ Wg,
+                                                 float *__restrict__ Mleaf, FmmDev f, int wsm)
+{
+    extern __shared__ __align__(16) float q[];  // [C][BB], then W [C][NR] when wsm
+    const int by = blockIdx.y, bx0 = blockIdx.x * BB, s = f.s;
+    const float *Wt = Wg;
+    if (wsm) {
+        float *Ws = q + f.C * BB;
+        const int n = f.C * f.NR;
+        for (int i = threadIdx.x * 4; i < n; i += blockDim.x * 4)
+            *reinterpret_cast<float4 *>(&Ws[i]) = __ldg(reinterpret_cast<const float4 *>(&Wg[i]));
+        Wt = Ws;
+    }
+    for (int i = threadIdx.x; i < f.C * BB; i += blockDim.x) {
+        const int b = i % BB, c = i / BB;
+        const int x = (bx0 + b) * s + c % s, y = by * s + (c / s) % s, z = c / (s * s);
+        q[i] = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < f.NR; k += blockDim.x) {
+        float acc[BB];
+#pragma unroll
+        for (int b = 0; b < BB; b++) acc[b] = 0.f;
+#pragma unroll 4
+        for (int c = 0; c < f.C; c++) {
+            const float w = Wt[(long long)c * f.NR + k];
+            const float4 qa = *reinterpret_cast<const float4 *>(&q[c * BB]);
+            const float4 qb = *reinterpret_cast<const float4 *>(&q[c * BB + 4]);
+            acc[0] = fmaf(w, qa.x, acc[0]);
+            acc[1] = fmaf(w, qa.y, acc[1]);
+            acc[2] = fmaf(w, qa.z, acc[2]);
+            acc[3] = fmaf(w, qa.w, acc[3]);
+            acc[4] = fmaf(w, qb.x, acc[4]);
+            acc[5] = fmaf(w, qb.y, acc[5]);
+            acc[6] = fmaf(w, qb.z, acc[6]);
+            acc[7] = fmaf(w, qb.w, acc[7]);
+        }
+#pragma unroll
+        for (int b = 0; b < BB; b++)
+            if (bx0 + b < f.nb) Mleaf[((long long)by * f.nb + bx0 + b) * f.NR + k] = acc[b];
+    }
+}
+
+// M2M: CTA per parent box, thread per (child c, output coefficient k).  The
+// four child operators (parity blocks only, [c][blk][j][k]) and the children's
+// expansions are staged in shared memory with one wave of bulk loads; the four
+// child contributions are summed in a fixed order.
+__device__ __forceinline__ int blk_base(int c, int NE, int NO, int blk)
+{
+    return c * (NE * NE + NO * NO) + (blk ? NE * NE : 0);
+}
+
+__global__ void k_m2m_c(float *__restrict__ Mall, const float *__restrict__ Tb, long long off_p, long long off_c,
+                        int np, FmmDev f)
+{
+    extern __shared__ __align__(16) float smb[];
+    const int NE = f.NE, NO = f.NR - f.NE;
+    const int tsz = 4 * (NE * NE + NO * NO);
+    const int KT = blockDim.x / 4;            // threads per child
+    float *Ts = smb;                          // [4][blocks]
+    float *Mc = smb + tsz;                    // [4][NR]
+    float *red = Mc + 4 * f.NR;               // [4][KT]
+    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    const int box = blockIdx.x, bx = box % np, by = box / np, nc = 2 * np;
+    for (int i = threadIdx.x; i < 4 * f.NR; i += blockDim.x) {
+        const int c = i / f.NR, j = i % f.NR;
+        const int cx = 2 * bx + (c & 1), cy = 2 * by + (c >> 1);
+        Mc[i] = Mall[(off_c + (long long)cy * nc + cx) * f.NR + j];
+    }
+    __syncthreads();
+    const int c = threadIdx.x / KT, k = threadIdx.x % KT;
+    float acc = 0.f;
+    if (k < f.NR) {
+        const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+        const float *T = Ts + blk_base(c, NE, NO, blk);
+        const float *m = Mc + c * f.NR + boff;
+#pragma unroll 8
+        for (int j = 0; j < NB; j++) acc = fmaf(T[j * NB + kk], m[j], acc);
+    }
+    red[c * KT + k] = acc;
+    __syncthreads();
+    if (c == 0 && k < f.NR)
+        Mall[(off_p + box) * f.NR + k] = (red[k] + red[KT + k]) + (red[2 * KT + k] + red[3 * KT + k]);
+}
+
+// M2L, all levels >= 2 in one launch.  CTA = 32 targets of one (level, parity
+// class) x one parity block of k x one of NSPLIT groups of 3 of the class's 27
+// offsets (blockIdx.z; each group writes its own partial locals, summed in a
+// fixed order by the downward pass).  Lane <-> target, warp <-> 16
+// consecutive k.  Per offset the operator block and the 32 source expansions
+// are staged in shared memory (odd row pitch: conflict-free per-lane reads);
+// the operator is read as warp-uniform float4 broadcasts, 16 FMAs per source
+// coefficient per lane.
+__global__ void __launch_bounds__(32 * M2L_WARPS) k_m2l_split(const float *__restrict__ Mall,
+                                                              float *__restrict__ Lpart,
+                                                              const float *__restrict__ Tm2l,
+                                                              const int4 *__restrict__ items,
+                                                              const long long *__restrict__ lev_off, FmmDev f,
+                                                              int KP0, int KP1, int NBmax, long long part_stride)
+{
+    extern __shared__ __align__(16) float sm2[];
+    const int4 it = items[blockIdx.x];
+    const int lev = it.x, px = it.y & 1, py = it.y >> 1;
+    const int blk = blockIdx.y, grp = blockIdx.z;
+    const int KP = blk ? KP1 : KP0;
+    const int KPmax = max(KP0, KP1);
+    const int NB = blk ? (f.NR - f.NE) : f.NE;
+    const int NBp = NB | 1;
+    const int boff = blk ? f.NE : 0;
+    float *Ts = sm2;                     // [NB][KP]
+    float *Ms = sm2 + NBmax * KPmax;     // [32][NBp]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = 1 << lev, nh = n >> 1;
+    const long long off = lev_off[lev];
+    const int k0 = warp * KW;
+    const bool wactive = k0 < NB;
+    const int ti = it.z + lane;
+    const bool tvalid = ti < nh * nh;
+    const int tx = 2 * (ti % nh) + px, ty = 2 * (ti / nh) + py;
+
+    float acc[KW];
+#pragma unroll
+    for (int i = 0; i < KW; i++) acc[i] = 0.f;
+
+    int idx = 0;
+    for (int oy = py - 3; oy <= py + 2; oy++)
+        for (int ox = px - 3; ox <= px + 2; ox++) {
+            if (max(abs(ox), abs(oy)) < 2) continue;
+            const int mine = (idx++ / (27 / NSPLIT)) == grp;
+            if (!mine) continue;
+            const int o = (oy + 3) * 7 + (ox + 3);
+            const float *Tg = Tm2l + ((long long)o * 2 + blk) * NBmax * KPmax;
+            __syncthreads();
+            for (int i = threadIdx.x * 4; i < NB * KP; i += blockDim.x * 4)
+                *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tg[i]));
+            for (int i = threadIdx.x; i < 32 * NB; i += blockDim.x) {
+                const int t = i / NB, j = i % NB;
+                const int tj = it.z + t;
+                const int ux = 2 * (tj % nh) + px - ox, uy = 2 * (tj / nh) + py - oy;
+                const bool ok = tj < nh * nh && ux >= 0 && uy >= 0 && ux < n && uy < n;
+                Ms[t * NBp + j] = ok ? __ldg(&Mall[(off + (long long)uy * n + ux) * f.NR + boff + j]) : 0.f;
+            }
+            __syncthreads();
+            if (!wactive) continue;
+            const float *mrow = Ms + lane * NBp;
+#pragma unroll 2
+            for (int j = 0; j < NB; j++) {
+                const float m = mrow[j];
+                const float4 *tr = reinterpret_cast<const float4 *>(&Ts[j * KP + k0]);
+#pragma unroll
+                for (int v = 0; v < KW / 4; v++) {
+                    const float4 t = tr[v];
+                    acc[4 * v + 0] = fmaf(t.x, m, acc[4 * v + 0]);
+                    acc[4 * v + 1] = fmaf(t.y, m, acc[4 * v + 1]);
+                    acc[4 * v + 2] = fmaf(t.z, m, acc[4 * v + 2]);
+                    acc[4 * v + 3] = fmaf(t.w, m, acc[4 * v + 3]);
+                }
+            }
+        }
+    if (!(wactive && tvalid)) return;
+    float *Lt = Lpart + grp * part_stride + (off + (long long)ty * n + tx) * f.NR + boff;
+#pragma unroll
+    for (int i = 0; i < KW; i++)
+        if (k0 + i < NB) Lt[k0 + i] = acc[i];
+}
+
+// M2L for low orders, all levels >= 2 in one launch: every operator block of
+// the 49 offset slots stays resident in shared memory (P <= 5).  CTA = 32
+// targets of one (level, parity class) x 8 warps; warp w takes offsets
+// w, w+8, w+16, w+24 of the class's 27; lane <-> target.  Each lane keeps its
+// source expansion and both parity blocks of its partial local in registers
+// and reads the operator rows as warp-uniform float2 broadcasts.  The 8 warps'
+// partials are summed in a fixed order in shared memory; the result is the
+// complete M2L local (one partial buffer).
+constexpr int RES_WARPS = 8;
+
+template <int NR_, int NE_>
+__global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restrict__ Mall, float *__restrict__ Lout,
+                                                            const float *__restrict__ Tc, const int4 *__restrict__ items,
+                                                            const long long *__restrict__ lev_off, FmmDev f)
+{
+    constexpr int NO_ = NR_ - NE_;
+    constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
+    extern __shared__ __align__(16) float sr[];
+    float *Ts = sr;                           // [49][OSZ], reused as [RES_WARPS][32][NR_ + 1]
+    float *red = sr;
+    for (int i = threadIdx.x * 4; i < 49 * OSZ; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tc[i]));
+    const int4 it = items[blockIdx.x];
+    const int lev = it.x, px = it.y & 1, py = it.y >> 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n = 1 << lev, nh = n >> 1;
+    const long long off = lev_off[lev];
+    const int ti = it.z + lane;
+    const bool tvalid = ti < nh * nh;
+    const int tx = 2 * (ti % nh) + px, ty = 2 * (ti / nh) + py;
+    // this warp's offsets (w, w+8, ...) of the class's 27, in class order
+    int ox_l[4], oy_l[4], no = 0;
+    {
+        int idx = 0;
+        for (int oy = py - 3; oy <= py + 2; oy++)
+            for (int ox = px - 3; ox <= px + 2; ox++) {
+                if (max(abs(ox), abs(oy)) < 2) continue;
+                if ((idx++ % RES_WARPS) == warp && no < 4) {
+                    ox_l[no] = ox;
+                    oy_l[no] = oy;
+                    no++;
+                }
+            }
+    }
+    float acc[NR_];
+#pragma unroll
+    for (int k = 0; k < NR_; k++) acc[k] = 0.f;
+    float m[NR_], mn[NR_];
+    auto fetch = [&](int q, float *dst) {
+        const int sx = tx - ox_l[q], sy = ty - oy_l[q];
+        const bool ok = tvalid && sx >= 0 && sy >= 0 && sx < n && sy < n;
+        const float2 *ms = reinterpret_cast<const float2 *>(Mall + (off + (long long)(ok ? sy : 0) * n + (ok ? sx : 0)) * NR_);
+#pragma unroll
+        for (int v = 0; v < NR_ / 2; v++) {
+            const float2 u = ok ? __ldg(&ms[v]) : make_float2(0.f, 0.f);
+            dst[2 * v] = u.x;
+            dst[2 * v + 1] = u.y;
+        }
+    };
+    if (no > 0) fetch(0, m);
+    __syncthreads();
+#pragma unroll 1
+    for (int q = 0; q < 4; q++) {
+        if (q >= no) break;
+        if (q + 1 < no) fetch(q + 1, mn);
+        const float *T = Ts + ((oy_l[q] + 3) * 7 + (ox_l[q] + 3)) * OSZ;
+#pragma unroll
+        for (int j = 0; j < NE_; j++) {
+            const float2 *row = reinterpret_cast<const float2 *>(T + j * NE_);
+#pragma unroll
+            for (int v = 0; v < NE_ / 2; v++) {
+                const float2 t = row[v];
+                acc[2 * v] = fmaf(t.x, m[j], acc[2 * v]);
+                acc[2 * v + 1] = fmaf(t.y, m[j], acc[2 * v + 1]);
+            }
+        }
+        T += NE_ * NE_;
+#pragma unroll
+        for (int j = 0; j < NO_; j++) {
+            const float2 *row = reinterpret_cast<const float2 *>(T + j * NO_);
+#pragma unroll
+            for (int v = 0; v < NO_ / 2; v++) {
+                const float2 t = row[v];
+                acc[NE_ + 2 * v] = fmaf(t.x, m[NE_ + j], acc[NE_ + 2 * v]);
+                acc[NE_ + 2 * v + 1] = fmaf(t.y, m[NE_ + j], acc[NE_ + 2 * v + 1]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < NR_; k++) m[k] = mn[k];
+    }
+    __syncthreads();  // operators no longer needed: the area becomes the reduction buffer
+    float *rw = red + (warp * 32 + lane) * (NR_ + 1);
+#pragma unroll
+    for (int k = 0; k < NR_; k++) rw[k] = acc[k];
+    __syncthreads();
+    // fixed-order sum over the warps: thread t handles (target, k) pairs
+    for (int e = threadIdx.x; e < 32 * NR_; e += blockDim.x) {
+        const int t = e / NR_, k = e % NR_;
+        const int tj = it.z + t;
+        if (tj >= nh * nh) continue;
+        float v = 0.f;
+#pragma unroll
+        for (int w = 0; w < RES_WARPS; w++) v += red[(w * 32 + t) * (NR_ + 1) + k];
+        const int ux = 2 * (tj % nh) + px, uy = 2 * (tj / nh) + py;
+        Lout[(off + (long long)uy * n + ux) * NR_ + k] = v;
+    }
+}
+
+// Downward pass of one level: L(child) = sum of the NSPLIT M2L partials of the
+// child (fixed order) + L2L of the final parent local.  CTA per parent box,
+// thread per (child c, coefficient k); operator blocks and the parent local
+// staged in shared memory.  np == 0 is level 2, which has no far-field
+// parent: its locals are the partial sums alone (CTA per box).
+__global__ void k_l2l_c(float *__restrict__ Lfin, const float *__restrict__ Lpart, const float *__restrict__ Tb,
+                        long long off_p, long long off_c, int nc, int np, long long part_stride, int nsplit, FmmDev f)
+{
+    extern __shared__ __align__(16) float smb[];
+    const int NE = f.NE, NO = f.NR - f.NE;
+    if (np == 0) {
+        const long long b = off_c + blockIdx.x;
+        for (int k = threadIdx.x; k < f.NR; k += blockDim.x) {
+            float v = 0.f;
+            for (int g = 0; g < nsplit; g++) v += Lpart[g * part_stride + b * f.NR + k];
+            Lfin[b * f.NR + k] = v;
+        }
+        return;
+    }
+    const int tsz = 4 * (NE * NE + NO * NO);
+    const int KT = blockDim.x / 4;
+    float *Ts = smb;          // [4][blocks]
+    float *Lp = smb + tsz;    // [NR]
+    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    const int pb = blockIdx.x;
+    for (int i = threadIdx.x; i < f.NR; i += blockDim.x) Lp[i] = Lfin[(off_p + pb) * (long long)f.NR + i];
+    __syncthreads();
+    const int c = threadIdx.x / KT, k = threadIdx.x % KT;
+    if (k >= f.NR) return;
+    const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+    const float *T = Ts + blk_base(c, NE, NO, blk);
+    const float *lp = Lp + boff;
+    float acc = 0.f;
+#pragma unroll 8
+    for (int j = 0; j < NB; j++) acc = fmaf(T[j * NB + kk], lp[j], acc);
+    const int cx = 2 * (pb % np) + (c & 1), cy = 2 * (pb / np) + (c >> 1);
+    const long long b = off_c + (long long)cy * nc + cx;
+    float v = acc;
+    for (int g = 0; g < nsplit; g++) v += Lpart[g * part_stride + b * f.NR + k];
+    Lfin[b * f.NR + k] = v;
+}
+
+// Leaf kernel: L2P + exact P2P.  CTA = BB leaf boxes of one row; thread =
+// (box, target row y, layer z) holding the S targets of its row in registers.
+// For every source row of the 3x3 leaf neighbourhood the thread loads the 3S
+// charges and the 2S-entry near-field row G[|dz|][|dy|][.] into registers and
+// does 3S x S FMAs with compile-time indices |S + i - j|.
+template <int S, int BB>
+__global__ void __launch_bounds__(512) k_leaf(const float *__restrict__ rho, const float *__restrict__ Lleaf,
+                                               const float *__restrict__ Vt, const float *__restrict__ Gn,
+                                               float *__restrict__ phi, FmmDev f, int far)
+{
+    extern __shared__ __align__(16) float sl[];
+    const int Z = f.Z;
+    constexpr int W = (BB + 2) * S;        // charges per staged row
+    float *qn = sl;                        // [Z][3S][W]
+    float *g = qn + Z * 3 * S * W;         // [Z][2S][2S]
+    float *Lb = g + Z * 4 * S * S;         // [BB][NR]
+    const int by = blockIdx.y, bx0 = blockIdx.x * BB;
+    const int xs0 = bx0 * S - S, ys0 = by * S - S;
+    for (int i = threadIdx.x; i < Z * 3 * S * W; i += blockDim.x) {
+        const int xx = xs0 + i % W, yy = ys0 + (i / W) % (3 * S), zz = i / (W * 3 * S);
+        qn[i] = (xx >= 0 && yy >= 0 && xx < f.X && yy < f.Y) ? rho[((long long)zz * f.Y + yy) * f.X + xx] : 0.f;
+    }
+    for (int i = threadIdx.x; i < Z * 4 * S * S; i += blockDim.x) g[i] = Gn[i];
+    if (far)
+        for (int i = threadIdx.x; i < BB * f.NR; i += blockDim.x) {
+            const int b = i / f.NR;
+            Lb[i] = (bx0 + b < f.nb) ? Lleaf[((long long)by * f.nb + bx0 + b) * f.NR + i % f.NR] : 0.f;
+        }
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int b = t / (S * Z), r = t % (S * Z);
+    const int ly = r % S, lz = r / S;
+    float acc[S];
+#pragma unroll
+    for (int i = 0; i < S; i++) acc[i] = 0.f;
+    for (int zs = 0; zs < Z; zs++) {
+        const int dz = abs(zs - lz);
+        for (int ys = 0; ys < 3 * S; ys++) {
+            const int dy = abs(ys - ly - S);
+            const float *grow = g + (dz * 2 * S + dy) * 2 * S;
+            const float *qrow = qn + (zs * 3 * S + ys) * W + b * S;
+            float gr[2 * S], qr[3 * S];
+            if constexpr (S % 4 == 0) {
+#pragma unroll
+                for (int v = 0; v < 2 * S / 4; v++) {
+                    const float4 u = reinterpret_cast<const float4 *>(grow)[v];
+                    gr[4 * v] = u.x; gr[4 * v + 1] = u.y; gr[4 * v + 2] = u.z; gr[4 * v + 3] = u.w;
+                }
+#pragma unroll
+                for (int v = 0; v < 3 * S / 4; v++) {
+                    const float4 u = reinterpret_cast<const float4 *>(qrow)[v];
+                    qr[4 * v] = u.x; qr[4 * v + 1] = u.y; qr[4 * v + 2] = u.z; qr[4 * v + 3] = u.w;
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < 2 * S; v++) gr[v] = grow[v];
+#pragma unroll
+                for (int v = 0; v < 3 * S; v++) qr[v] = qrow[v];
+            }
+#pragma unroll
+            for (int j = 0; j < 3 * S; j++)
+#pragma unroll
+                for (int i = 0; i < S; i++) {
+                    const int d = (S + i - j) < 0 ? (j - S - i) : (S + i - j);
+                    acc[i] = fmaf(qr[j], gr[d], acc[i]);
+                }
+        }
+    }
+    if (far) {
+        const float *Lbb = Lb + b * f.NR;
+        const int c0 = lz * S * S + ly * S;
+        for (int k = 0; k < f.NR; k++) {
+            const float lk = Lbb[k];
+            const float *vrow = Vt + (long long)k * f.C + c0;
+            if constexpr (S % 4 == 0) {
+#pragma unroll
+                for (int v = 0; v < S / 4; v++) {
+                    const float4 u = __ldg(reinterpret_cast<const float4 *>(vrow) + v);
+                    acc[4 * v + 0] = fmaf(u.x, lk, acc[4 * v + 0]);
+                    acc[4 * v + 1] = fmaf(u.y, lk, acc[4 * v + 1]);
+                    acc[4 * v + 2] = fmaf(u.z, lk, acc[4 * v + 2]);
+                    acc[4 * v + 3] = fmaf(u.w, lk, acc[4 * v + 3]);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < S; i++) acc[i] = fmaf(__ldg(&vrow[i]), lk, acc[i]);
+            }
+        }
+    }
+    const int y = by * S + ly;
+    if (bx0 + b >= f.nb || y >= f.Y) return;
+#pragma unroll
+    for (int i = 0; i < S; i++) {
+        const int x = (bx0 + b) * S + i;
+        if (x < f.X) phi[((long long)lz * f.Y + y) * f.X + x] = acc[i];
+    }
 }
 
 __global__ void k_build_gn(float *__restrict__ Gn, int Z, int s, double dx, double dy, double dz)
@@ -261,6 +569,102 @@ int upload(mms_ctx *ctx, FmmPlan *pl, T **dst, const std::vector<T> &v)
     return MMS_OK;
 }
 
+
+// leaf-kernel specialisations: boxes per CTA, threads per CTA (0 = none)
+int leaf_bb(int S) { return S >= 8 ? 4 : 8; }
+
+int leaf_threads(const FmmDev &f)
+{
+    const int S = f.s;
+    if (S != 2 && S != 4 && S != 8 && S != 16) return 0;
+    const int t = leaf_bb(S) * S * f.Z;
+    return t <= 512 ? t : 0;
+}
+
+size_t leaf_smem(const FmmDev &f)
+{
+    const int S = f.s, B = leaf_bb(S), W = (B + 2) * S;
+    return ((size_t)f.Z * 3 * S * W + (size_t)f.Z * 4 * S * S + (size_t)B * f.NR) * sizeof(float);
+}
+
+int leaf_set_smem(int S, size_t bytes)
+{
+    cudaError_t e = cudaSuccess;
+    const int b = (int)bytes;
+    switch (S) {
+    case 2: e = cudaFuncSetAttribute(k_leaf<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
+    case 4: e = cudaFuncSetAttribute(k_leaf<4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
+    case 8: e = cudaFuncSetAttribute(k_leaf<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
+    case 16: e = cudaFuncSetAttribute(k_leaf<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
+    default: break;
+    }
+    if (e != cudaSuccess) {
+        mms_set_error("leaf kernel shared memory (%zu B): %s", bytes, cudaGetErrorString(e));
+        return MMS_ERR_ARG;
+    }
+    return MMS_OK;
+}
+
+int leaf_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float *Lleaf, const float *Vt,
+                const float *Gn, float *phi, int far, cudaStream_t st)
+{
+    const int t = leaf_threads(f);
+    const size_t sm = leaf_smem(f);
+    const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
+    switch (f.s) {
+    case 2: k_leaf<2, 8><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
+    case 4: k_leaf<4, 8><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
+    case 8: k_leaf<8, 4><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
+    case 16: k_leaf<16, 4><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
+    default:
+        mms_set_error("no leaf kernel for side %d", f.s);
+        return MMS_ERR_ARG;
+    }
+    return MMS_OK;
+}
+
+
+// resident-operator M2L specialisations: (NR, NE) for P = 1 .. 5
+#define MMS_M2L_RES_CASES(X) X(6, 4) X(12, 8) X(20, 12) X(30, 18) X(42, 24)
+
+int m2l_res_supported(int NR, int NE)
+{
+#define X(a, b) if (NR == a && NE == b) return 1;
+    MMS_M2L_RES_CASES(X)
+#undef X
+    return 0;
+}
+
+size_t m2l_res_smem(int NR, int NE)
+{
+    const int NO = NR - NE;
+    return std::max((size_t)49 * (NE * NE + NO * NO), (size_t)RES_WARPS * 32 * (NR + 1)) * sizeof(float);
+}
+
+int m2l_res_prepare(int NR, int NE)
+{
+    const int b = (int)m2l_res_smem(NR, NE);
+    cudaError_t e = cudaSuccess;
+#define X(a, c) if (NR == a && NE == c) e = cudaFuncSetAttribute(k_m2l_res<a, c>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    MMS_M2L_RES_CASES(X)
+#undef X
+    if (e != cudaSuccess) {
+        mms_set_error("M2L shared memory (%d B): %s", b, cudaGetErrorString(e));
+        return MMS_ERR_ARG;
+    }
+    return MMS_OK;
+}
+
+int m2l_res_launch(const FmmDev &f, int nitems, const float *Mall, float *Lout, const float *Tc, const int4 *items,
+                   const long long *lev, cudaStream_t st)
+{
+    const size_t sm = m2l_res_smem(f.NR, f.NE);
+#define X(a, c) if (f.NR == a && f.NE == c) { k_m2l_res<a, c><<<nitems, 32 * RES_WARPS, sm, st>>>(Mall, Lout, Tc, items, lev, f); return MMS_OK; }
+    MMS_M2L_RES_CASES(X)
+#undef X
+    mms_set_error("no resident M2L kernel for NR=%d", f.NR);
+    return MMS_ERR_ARG;
+}
 }  // namespace
 
 int fmm_default_leaf(int P, int X, int Y);
@@ -268,8 +672,8 @@ int fmm_default_leaf(int P, int X, int Y);
 int fmm_plan_create(mms_ctx *ctx)
 {
     const int P = ctx->s.fmm_order;
-    if (P < 1 || P > 12) {
-        mms_set_error("FMM order P must be 1..12 (got %d)", P);
+    if (P < 1 || P > 9) {
+        mms_set_error("FMM order P must be 1..9 (got %d)", P);
         return MMS_ERR_ARG;
     }
     int s = ctx->s.fmm_leaf;
@@ -318,20 +722,27 @@ int fmm_plan_create(mms_ctx *ctx)
     for (int k = 0; k < f.NR; k++)
         for (int c = 0; c < f.C; c++) {
             Wt[(size_t)c * f.NR + k] = (float)(W[(size_t)k * f.C + c] * dV);
-            Vt[(size_t)k * f.C + c] = (float)V[(size_t)c * f.NR + k];
+            Vt[(size_t)k * f.C + c] = (float)(V[(size_t)c * f.NR + k] / w);
         }
     // M2M / L2L, transposed to [j][k]
     const int NR = f.NR;
-    std::vector<float> Tm2m((size_t)4 * NR * NR), Tl2l((size_t)4 * NR * NR);
+    // M2M / L2L parity blocks, [c][blk][j][k]
+    const int NEb = f.NE, NOb = NR - f.NE;
+    const size_t cstride = (size_t)NEb * NEb + (size_t)NOb * NOb;
+    std::vector<float> Tm2m(4 * cstride), Tl2l(4 * cstride);
     for (int c = 0; c < 4; c++) {
         const double dxv = ((c & 1) - 0.5) / 2, dyv = ((c >> 1) - 0.5) / 2 * ay;
         const std::vector<double> a = fmmops::m2m(lay, dxv, dyv, 0.0);
         const std::vector<double> b = fmmops::l2l(lay, -dxv, -dyv, 0.0);
-        for (int k = 0; k < NR; k++)
-            for (int j = 0; j < NR; j++) {
-                Tm2m[((size_t)c * NR + j) * NR + k] = (float)a[(size_t)k * NR + j];
-                Tl2l[((size_t)c * NR + j) * NR + k] = (float)b[(size_t)k * NR + j];
-            }
+        for (int blk = 0; blk < 2; blk++) {
+            const int b0 = blk ? NEb : 0, NB = blk ? NOb : NEb;
+            const size_t base = c * cstride + (blk ? (size_t)NEb * NEb : 0);
+            for (int j = 0; j < NB; j++)
+                for (int k = 0; k < NB; k++) {
+                    Tm2m[base + (size_t)j * NB + k] = (float)a[(size_t)(b0 + k) * NR + (b0 + j)];
+                    Tl2l[base + (size_t)j * NB + k] = (float)b[(size_t)(b0 + k) * NR + (b0 + j)];
+                }
+        }
     }
     // M2L parity blocks, [o][blk][j][k padded]
     const int NB0 = f.NE, NB1 = NR - f.NE, NBmax = std::max(NB0, NB1);
@@ -361,6 +772,16 @@ int fmm_plan_create(mms_ctx *ctx)
                 for (int j = 0; j < NR; j++)
                     if ((k < f.NE) != (j < f.NE)) max_offblock = std::max(max_offblock, fabs(T[(size_t)k * NR + j]));
         }
+    std::vector<float> Tm2lc((size_t)49 * ((size_t)NB0 * NB0 + (size_t)NB1 * NB1), 0.f);
+    for (int o = 0; o < 49; o++)
+        for (int blk = 0; blk < 2; blk++) {
+            const int NB = blk ? NB1 : NB0, KP = pl->KPb[blk];
+            const float *src = &Tm2l[((size_t)o * 2 + blk) * NBmax * KPmax];
+            float *dst = &Tm2lc[(size_t)o * ((size_t)NB0 * NB0 + (size_t)NB1 * NB1) + (blk ? (size_t)NB0 * NB0 : 0)];
+            for (int j = 0; j < NB; j++)
+                for (int k = 0; k < NB; k++) dst[(size_t)j * NB + k] = src[(size_t)j * KP + k];
+        }
+    pl->m2l_resident = m2l_res_supported(NR, f.NE);
     if (max_offblock > 1e-9) {
         delete pl;
         ctx->fmm = nullptr;
@@ -390,6 +811,7 @@ int fmm_plan_create(mms_ctx *ctx)
     if (!st) st = upload(ctx, pl, &pl->Tm2m, Tm2m);
     if (!st) st = upload(ctx, pl, &pl->Tl2l, Tl2l);
     if (!st) st = upload(ctx, pl, &pl->Tm2l, Tm2l);
+    if (!st) st = upload(ctx, pl, &pl->Tm2lc, Tm2lc);
     if (!st) st = upload(ctx, pl, &pl->m2l_items, items);
     long long *lev_dev = nullptr;
     if (!st) st = upload(ctx, pl, &lev_dev, pl->lev_off);
@@ -402,13 +824,15 @@ int fmm_plan_create(mms_ctx *ctx)
         const size_t ncoef = (size_t)tot * NR;
         if (cudaMalloc((void **)&pl->Mall, ncoef * sizeof(float)) != cudaSuccess ||
             cudaMalloc((void **)&pl->Lall, ncoef * sizeof(float)) != cudaSuccess ||
+            cudaMalloc((void **)&pl->Lpart, NSPLIT * ncoef * sizeof(float)) != cudaSuccess ||
             cudaMalloc((void **)&pl->Gn, (size_t)Z * 4 * s * s * sizeof(float)) != cudaSuccess) {
             cudaFree(lev_dev);
             fmm_plan_destroy(ctx);
             mms_set_error("FMM plan: device allocation failed");
             return MMS_ERR_NOMEM;
         }
-        pl->bytes += 2 * ncoef * sizeof(float) + (size_t)Z * 4 * s * s * sizeof(float);
+        pl->bytes += (2 + NSPLIT) * ncoef * sizeof(float) + (size_t)Z * 4 * s * s * sizeof(float);
+        MMS_CUDA_TRY(cudaMemsetAsync(pl->Lpart, 0, NSPLIT * ncoef * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Mall, 0, ncoef * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Lall, 0, ncoef * sizeof(float), ctx->stream));
     }
@@ -416,15 +840,34 @@ int fmm_plan_create(mms_ctx *ctx)
                                                                             ctx->g.dz);
     MMS_LAUNCH_CHECK(ctx);
     pl->lev_dev = lev_dev;
-    const size_t m2l_smem = (size_t)NBmax * KPmax * sizeof(float);
-    if (m2l_smem > 48 * 1024)
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2l, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2l_smem));
+    const size_t m2ls_smem = ((size_t)NBmax * KPmax + 32 * (size_t)(NBmax | 1)) * sizeof(float);
+    if (m2ls_smem > 48 * 1024)
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2l_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2ls_smem));
+    if (pl->m2l_resident) MMS_TRY(m2l_res_prepare(NR, f.NE));
+    {
+        const size_t pm = (size_t)f.C * (BB + f.NR) * sizeof(float);
+        if (pm > 48 * 1024 && pm <= 160 * 1024)
+            MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pm));
+    }
+    {
+        const size_t tsz = 4 * cstride;
+        const int KT = ((NR + 31) / 32) * 32;
+        const size_t a1 = (tsz + 4 * (size_t)NR + 4 * (size_t)KT) * sizeof(float), a2 = (tsz + (size_t)NR) * sizeof(float);
+        if (a1 > 48 * 1024)
+            MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2m_c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a1));
+        if (a2 > 48 * 1024)
+            MMS_CUDA_TRY(cudaFuncSetAttribute(k_l2l_c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a2));
+    }
+    if (leaf_threads(f) > 0) {
+        const size_t lsm = leaf_smem(f);
+        if (lsm > 48 * 1024) MMS_TRY(leaf_set_smem(f.s, lsm));
+    }
 
-    // algorithmic work of one evaluation (FMA = 2 flops)
+    // algorithmic work of one evaluation (FMA = 2 flops), per stage
     const long long nleafb = (long long)f.nb * f.nb;
     double fl = 0;
-    fl += 2.0 * nleafb * f.C * NR;  // P2M
-    fl += 2.0 * nleafb * f.C * NR;  // L2P
+    pl->stage_flops[0] = 2.0 * nleafb * f.C * NR;  // P2M
+    pl->stage_flops[4] = 2.0 * nleafb * f.C * NR;  // L2P (P2P added below)
     long long m2l_pairs = 0;
     for (int l = 2; l <= f.L; l++) {
         const int n = 1 << l;
@@ -437,9 +880,11 @@ int fmm_plan_create(mms_ctx *ctx)
                             m2l_pairs++;
     }
     const double blk2 = (double)NB0 * NB0 + (double)NB1 * NB1;
-    fl += 2.0 * m2l_pairs * blk2;
-    for (int l = 2; l < f.L; l++) fl += 2.0 * 4.0 * (double)(1 << l) * (1 << l) * blk2;           // M2M
-    for (int l = 3; l <= f.L; l++) fl += 2.0 * (double)(1 << l) * (1 << l) * blk2;               // L2L
+    pl->stage_flops[2] = 2.0 * m2l_pairs * blk2;
+    pl->stage_flops[1] = 0;
+    for (int l = 2; l < f.L; l++) pl->stage_flops[1] += 2.0 * 4.0 * (double)(1 << l) * (1 << l) * blk2;
+    pl->stage_flops[3] = 0;
+    for (int l = 3; l <= f.L; l++) pl->stage_flops[3] += 2.0 * (double)(1 << l) * (1 << l) * blk2;
     // P2P: each target cell against every cell of its 3x3 leaf neighbourhood inside the grid
     long long pairs = 0;
     for (int by = 0; by < f.nb; by++)
@@ -451,7 +896,11 @@ int fmm_plan_create(mms_ctx *ctx)
             const int sy = std::max(0, std::min(f.Y, (by + 2) * s) - std::max(0, (by - 1) * s));
             pairs += (long long)tx * ty * Z * sx * sy * Z;
         }
-    fl += 2.0 * pairs;
+    pl->stage_flops[4] += 2.0 * pairs;
+    if (f.L < 2)
+        for (int i = 0; i < 4; i++) pl->stage_flops[i] = 0;
+    if (f.L < 2) pl->stage_flops[4] = 2.0 * pairs;
+    for (int i = 0; i < 5; i++) fl += pl->stage_flops[i];
     pl->flops = fl;
     pl->p2p_pairs = pairs;
     pl->m2l_pairs = m2l_pairs;
@@ -464,8 +913,8 @@ void fmm_plan_destroy(mms_ctx *ctx)
     FmmPlan *pl = ctx->fmm;
     if (!pl) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Gn, pl->Mall, pl->Lall, pl->m2l_items,
-                 pl->lev_dev};
+    void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Tm2lc, pl->Gn, pl->Mall, pl->Lall, pl->Lpart,
+                 pl->m2l_items, pl->lev_dev};
     for (void *p : b)
         if (p) cudaFree(p);
     delete pl;
@@ -473,6 +922,15 @@ void fmm_plan_destroy(mms_ctx *ctx)
 }
 
 size_t fmm_plan_bytes(const mms_ctx *ctx) { return ctx->fmm ? ctx->fmm->bytes : 0; }
+
+// optional per-stage CUDA events (mms_fmm_stage_times): stage 0 P2M, 1 M2M,
+// 2 M2L, 3 L2L, 4 L2P+P2P; each mark records the end of that stage
+static thread_local cudaEvent_t *g_stage_ev = nullptr;
+
+static void stage_mark(mms_ctx *ctx, int stage)
+{
+    if (g_stage_ev) cudaEventRecord(g_stage_ev[stage + 1], ctx->stream);
+}
 
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
 {
@@ -483,34 +941,65 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
     }
     const FmmDev &f = pl->d;
     const int far = f.L >= 2;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    const bool tuned = leaf_threads(f) > 0;
+    const long long part_stride = pl->nbox_total * f.NR;
+    const int thr = ((f.NR + 31) / 32) * 32;
     if (far) {
         const long long leaf_off = pl->lev_off[f.L];
-        k_p2m<<<f.nb * f.nb, 128, f.C * sizeof(float), ctx->stream>>>(rho, pl->Wt, pl->Mall + leaf_off * f.NR, f);
+        const int wsm = (f.C * f.NR) % 4 == 0 && (size_t)f.C * (BB + f.NR) * sizeof(float) <= 160 * 1024;
+        k_p2m_row<<<dim3(div_up(nbx, BB), nby), 128, (size_t)f.C * (BB + (wsm ? f.NR : 0)) * sizeof(float),
+                    ctx->stream>>>(rho, pl->Wt, pl->Mall + leaf_off * f.NR, f, wsm);
         MMS_LAUNCH_CHECK(ctx);
+        stage_mark(ctx, 0);
+        const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
+        const int KT = ((f.NR + 31) / 32) * 32;
         for (int l = f.L - 1; l >= 2; l--) {
             const int np = 1 << l;
-            k_m2m<<<np * np, ((f.NR + 31) / 32) * 32, 0, ctx->stream>>>(pl->Mall, pl->Tm2m, pl->lev_off[l],
-                                                                       pl->lev_off[l + 1], np, f);
+            k_m2m_c<<<np * np, 4 * KT, (tsz + 4 * (size_t)f.NR + 4 * (size_t)KT) * sizeof(float), ctx->stream>>>(
+                pl->Mall, pl->Tm2m, pl->lev_off[l], pl->lev_off[l + 1], np, f);
             MMS_LAUNCH_CHECK(ctx);
+            stage_mark(ctx, 1);
         }
         const int NBmax = std::max(f.NE, f.NR - f.NE);
         const int KPmax = std::max(pl->KPb[0], pl->KPb[1]);
-        dim3 grid(pl->n_m2l_items, 2);
-        k_m2l<<<grid, 32 * M2L_WARPS, (size_t)NBmax * KPmax * sizeof(float), ctx->stream>>>(
-            pl->Mall, pl->Lall, pl->Tm2l, pl->m2l_items, pl->lev_dev, f, pl->KPb[0], pl->KPb[1], NBmax);
+        const size_t sm = ((size_t)NBmax * KPmax + 32 * (size_t)(NBmax | 1)) * sizeof(float);
+        int nsplit = NSPLIT;
+        if (pl->m2l_resident) {
+            MMS_TRY(m2l_res_launch(f, pl->n_m2l_items, pl->Mall, pl->Lpart, pl->Tm2lc, pl->m2l_items, pl->lev_dev,
+                                   ctx->stream));
+            nsplit = 1;
+        } else {
+            k_m2l_split<<<dim3(pl->n_m2l_items, 2, NSPLIT), 32 * M2L_WARPS, sm, ctx->stream>>>(
+                pl->Mall, pl->Lpart, pl->Tm2l, pl->m2l_items, pl->lev_dev, f, pl->KPb[0], pl->KPb[1], NBmax,
+                part_stride);
+        }
+        MMS_LAUNCH_CHECK(ctx);
+        stage_mark(ctx, 2);
+        k_l2l_c<<<16, thr, 0, ctx->stream>>>(pl->Lall, pl->Lpart, pl->Tl2l, 0, pl->lev_off[2], 4, 0, part_stride,
+                                             nsplit, f);
         MMS_LAUNCH_CHECK(ctx);
         for (int l = 3; l <= f.L; l++) {
-            const int nc = 1 << l;
-            k_l2l<<<nc * nc, ((f.NR + 31) / 32) * 32, 0, ctx->stream>>>(pl->Lall, pl->Tl2l, pl->lev_off[l - 1],
-                                                                       pl->lev_off[l], nc, f);
+            const int nc = 1 << l, np = nc / 2;
+            k_l2l_c<<<np * np, 4 * KT, (tsz + (size_t)f.NR) * sizeof(float), ctx->stream>>>(
+                pl->Lall, pl->Lpart, pl->Tl2l, pl->lev_off[l - 1], pl->lev_off[l], nc, np, part_stride, nsplit, f);
             MMS_LAUNCH_CHECK(ctx);
         }
+        stage_mark(ctx, 3);
     }
-    const size_t smem = ((size_t)f.Z * 9 * f.s * f.s + (size_t)f.Z * 4 * f.s * f.s + f.NR) * sizeof(float);
-    const int threads = ((f.C + 31) / 32) * 32;
-    k_l2p_p2p<<<f.nb * f.nb, threads, smem, ctx->stream>>>(rho, pl->Lall + pl->lev_off[f.L] * f.NR, pl->Vt, pl->Gn,
-                                                          phi, f, far);
-    MMS_LAUNCH_CHECK(ctx);
+    if (tuned) {
+        MMS_TRY(leaf_launch(f, nbx, nby, rho, pl->Lall + pl->lev_off[f.L] * f.NR, pl->Vt, pl->Gn, phi, far,
+                            ctx->stream));
+        MMS_LAUNCH_CHECK(ctx);
+        stage_mark(ctx, 4);
+    } else {
+        const size_t smem = ((size_t)f.Z * 9 * f.s * f.s + (size_t)f.Z * 4 * f.s * f.s + f.NR) * sizeof(float);
+        const int threads = ((f.C + 31) / 32) * 32;
+        k_l2p_p2p<<<f.nb * f.nb, threads, smem, ctx->stream>>>(rho, pl->Lall + pl->lev_off[f.L] * f.NR, pl->Vt,
+                                                              pl->Gn, phi, f, far);
+        MMS_LAUNCH_CHECK(ctx);
+        stage_mark(ctx, 4);
+    }
     return MMS_OK;
 }
 
@@ -522,7 +1011,7 @@ int fmm_default_leaf(int P, int X, int Y)
     return P <= 4 ? 4 : 8;
 }
 
-extern "C" int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double *flops,
+extern "C" int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double stage_flops[5],
                             long long *p2p_pairs, long long *m2l_pairs)
 {
     if (!ctx || !ctx->fmm) {
@@ -533,8 +1022,39 @@ extern "C" int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *ord
     if (levels) *levels = pl->d.L;
     if (leaf) *leaf = pl->d.s;
     if (order) *order = pl->d.P;
-    if (flops) *flops = pl->flops;
+    if (stage_flops)
+        for (int i = 0; i < 5; i++) stage_flops[i] = pl->stage_flops[i];
     if (p2p_pairs) *p2p_pairs = pl->p2p_pairs;
     if (m2l_pairs) *m2l_pairs = pl->m2l_pairs;
     return MMS_OK;
+}
+
+extern "C" int mms_fmm_stage_times(mms_ctx *ctx, const float *rho, float *phi, int reps, double ms[5])
+{
+    if (!ctx || !ctx->fmm || !rho || !phi || reps < 1 || !ms) {
+        mms_set_error("mms_fmm_stage_times: bad argument or no FMM plan");
+        return MMS_ERR_ARG;
+    }
+    cudaEvent_t ev[6];
+    for (int i = 0; i < 6; i++) MMS_CUDA_TRY(cudaEventCreate(&ev[i]));
+    for (int i = 0; i < 5; i++) ms[i] = 0.0;
+    int st = launch_potential_fmm(ctx, rho, phi);  // warm-up
+    for (int r = 0; r < reps && st == MMS_OK; r++) {
+        cudaEventRecord(ev[0], ctx->stream);
+        for (int i = 1; i < 6; i++) cudaEventRecord(ev[i], ctx->stream);  // stages that do not run keep 0 width
+        g_stage_ev = ev;
+        st = launch_potential_fmm(ctx, rho, phi);
+        g_stage_ev = nullptr;
+        cudaEventSynchronize(ev[5]);
+        float prev = 0.f;
+        for (int i = 1; i < 6; i++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[0], ev[i]);
+            if (t < prev) t = prev;
+            ms[i - 1] += (t - prev) / reps;
+            prev = t;
+        }
+    }
+    for (int i = 0; i < 6; i++) cudaEventDestroy(ev[i]);
+    return st;
 }

@@ -105,6 +105,7 @@ SIGNATURES = {
     "mms_march": (_I, [_VP, ctypes.POINTER(Controller), _D, _D, ctypes.POINTER(Record), _I, ctypes.POINTER(_I),
                        MARCH_CB, _VP]),
     "mms_diag_fma_tflops": (_I, [_I, ctypes.POINTER(_D)]),
+    "mms_fmm_stage_times": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_D)]),
     "mms_fmm_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D),
                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
 }
@@ -152,12 +153,20 @@ def fma_tflops(reps=20):
 def fmm_stats(ctx):
     """FMM plan of a context: levels, leaf, order, flops per evaluation, pair counts"""
     L, s, P = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-    fl = ctypes.c_double()
+    fl = (ctypes.c_double * 5)()
     pp, mp = ctypes.c_longlong(), ctypes.c_longlong()
-    _check(load().mms_fmm_info(ctx.h, ctypes.byref(L), ctypes.byref(s), ctypes.byref(P), ctypes.byref(fl),
+    _check(load().mms_fmm_info(ctx.h, ctypes.byref(L), ctypes.byref(s), ctypes.byref(P), fl,
                                ctypes.byref(pp), ctypes.byref(mp)))
-    return dict(levels=L.value, leaf=s.value, order=P.value, flops=fl.value, p2p_pairs=pp.value,
-                m2l_pairs=mp.value)
+    stages = dict(zip(("p2m", "m2m", "m2l", "l2l", "l2p_p2p"), list(fl)))
+    return dict(levels=L.value, leaf=s.value, order=P.value, flops=float(sum(fl)), stage_flops=stages,
+                p2p_pairs=pp.value, m2l_pairs=mp.value)
+
+
+def fmm_stage_times(ctx, rho, phi, reps=10):
+    """per-stage device ms of the FMM potential: P2M, M2M, M2L, L2L, L2P+P2P"""
+    out = (ctypes.c_double * 5)()
+    _check(load().mms_fmm_stage_times(ctx.h, _ptr(rho), _ptr(phi), reps, out))
+    return dict(zip(("p2m", "m2m", "m2l", "l2l", "l2p_p2p"), list(out)))
 
 
 def make_params(Ms=8.6e5, Aexch=1.3e-11, alpha=0.5, gamma=2.21e5, mu0=4e-7 * np.pi, demag=True, exchange=True,
