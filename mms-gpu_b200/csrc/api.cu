@@ -719,8 +719,8 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
                 continue;
             }
             rejects = 0;
-            dt = 1e-14 / torque / 2;
-            t = t + ts[TIME_DT];
+            t = t + dt;                   // the step just taken
+            dt = 1e-14 / torque / 2;      // ode_functions.cpp:298-299
             tindex++;
             E = E2;
             if (record(dt, E2, torque)) break;

@@ -50,23 +50,6 @@ int rk4_step(const fptype t, const fptype dt, fptype *t2,
              const int demag, const int exchange, const int external, const int use_fmm,
              const int normalize, const int use_gpu, const int verbosity);
 
-/* CPU-only stand-ins for the reference's CUDA-side symbols.  The harness only
- * ever runs use_gpu == 0, so these are never reached on a correct call. */
-void checkCUDAError(const char *msg) { (void)msg; }
-int calc_potential_exact_gpu(const fptype *, const int, const int, const int,
-                             const fptype, const fptype, const fptype, fptype *)
-{
-    fprintf(stderr, "mmsref_harness: GPU direct path is not part of the CPU oracle\n");
-    return EXIT_FAILURE;
-}
-int fmm_gpu(const Box *const, const Cmpx *const, fptype *, const unsigned int, const int,
-            const int, const int, const int, const fptype, const fptype, const fptype,
-            const int, const int, const int)
-{
-    fprintf(stderr, "mmsref_harness: GPU FMM path is not part of the CPU oracle\n");
-    return EXIT_FAILURE;
-}
-
 static std::map<std::string, std::string> g_args;
 
 static const char *arg_s(const char *k, const char *def = nullptr)

@@ -120,7 +120,39 @@ def main():
     Mf, rows = ref.march(mat, M, (X, Y, Z), d, finaltime=2e-12, timestep=1e-14)
     np.savez_compressed(os.path.join(HERE, "march_8x8x3.npz"), M0=M, material=mat, M_final=Mf, dynamics=rows,
                         dims=(X, Y, Z), d=d, finaltime=2e-12, timestep=1e-14, entry="time_marching")
+    # 6. the reference's own driver main.cpp (CPU build, oracle/_ref/main_ref):
+    #    its dynamics.dat for two short runs, for the drop-in test of main.cpp
+    #    linked against libmms_refapi.so
+    main_ref = os.path.join(os.path.dirname(ref.REF_HARNESS), "main_ref")
+    if os.path.exists(main_ref):
+        import subprocess
+        import tempfile
+        rec = {"entry": "main.cpp -> time_marching"}
+        for name, args in DROPIN_RUNS.items():
+            with tempfile.TemporaryDirectory() as td:
+                subprocess.run([main_ref] + args, cwd=td, check=True, stdin=subprocess.DEVNULL,
+                               stdout=subprocess.DEVNULL)
+                rows = []
+                with open(os.path.join(td, args[15], "dynamics.dat")) as f:
+                    for line in f:
+                        parts = line.replace(",", " ").split()
+                        if len(parts) == 9:
+                            rows.append([float(v) for v in parts])
+                rec[name] = np.array(rows)
+                rec[name + "_args"] = np.array(args)
+        np.savez_compressed(os.path.join(HERE, "dropin_main_16x16x3.npz"), **rec)
     print("wrote fixtures to", HERE)
+
+
+# main.cpp positional arguments (main.cpp:49-70): image P finaltime timestep
+# width height depth xdim ydim zdim demag exchange external use_fmm use_gpu
+# sim_name seed IC
+DROPIN_RUNS = {
+    "sd": ["dummy.png", "3", "3e-11", "1e-14", "80e-9", "80e-9", "15e-9", "16", "16", "3", "1", "1", "0", "0",
+           "0", "sim", "2010", "0"],
+    "vortex_ext": ["dummy.png", "3", "2e-11", "1e-14", "80e-9", "80e-9", "15e-9", "16", "16", "3", "1", "1", "1",
+                   "0", "0", "sim", "2010", "1"],
+}
 
 
 if __name__ == "__main__":
