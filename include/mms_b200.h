@@ -181,6 +181,24 @@ int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double 
  * ctx's stream between the stage launches; rho/phi are device arrays. */
 int mms_fmm_stage_times(mms_ctx *ctx, const float *rho, float *phi, int reps, double ms[5]);
 
+/* allocation-free exact potential -------------------------------------------- */
+/* No counterpart in the reference.  The exact direct-sum potential for callers
+ * that cannot allocate device memory (a host whose pool allocator owns the
+ * device memory, code running during CUDA graph capture, a loop that must not
+ * take the allocation lock): no context, and no cudaMalloc/cudaFree or other
+ * allocating call.  The scratch table lives in a fixed 4 MiB array inside the
+ * library that each GPU which loads the library holds until exit; grids are
+ * limited to xdim*ydim*zdim <= 1,048,576 cells and xdim <= 2048 (MMS_ERR_ARG
+ * beyond).  rho/phi are device arrays; the work is queued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream).  The first call on each device
+ * performs a one-time set-up (the table's device address, a kernel attribute)
+ * with that device current; make that first call before any stream capture.
+ * All calls share the one table, which keeps the last call's contents: calls
+ * that overlap on the GPU (different streams, or different host threads on one
+ * device) race and must be serialised by the caller. */
+int mms_potential_direct_noalloc(const float *rho, float *phi, int xdim, int ydim, int zdim,
+                                 double dx, double dy, double dz, void *stream);
+
 /* diagnostics ---------------------------------------------------------------- */
 /* FP32 FMA throughput of the current device in TFLOP/s (a microbenchmark of
  * `reps` launches, one wave of 8 CTAs per SM): the roofline denominator of the

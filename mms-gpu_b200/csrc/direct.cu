@@ -210,3 +210,71 @@ int launch_potential_direct(mms_ctx *ctx, const float *rho, float *phi)
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the exact potential.
+//
+// For callers that cannot call cudaMalloc: a host that has handed the device
+// memory to its own pool allocator, code that runs while a CUDA graph is being
+// captured (where allocation is not permitted), or a latency-critical loop that
+// must not take the driver's allocation lock.  The direct sum's only scratch
+// is its table G[|dz|][|dy|][|dx|] = dV/|r|; here it lives in a fixed array in
+// the library's own device memory (module global), so a call needs nothing but
+// the caller's input and output buffers.
+//
+// Limit: X*Y*Z <= MMS_NOALLOC_MAX_CELLS (1,048,576 cells, a 4 MiB table that
+// every GPU which loads the library holds until the process exits) and
+// xdim <= 2048.
+constexpr long long MMS_NOALLOC_MAX_CELLS = 1LL << 20;
+static __device__ __align__(256) float g_noalloc_gtab[MMS_NOALLOC_MAX_CELLS];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+float *g_noalloc_ptr[NOALLOC_MAX_DEVICES];   // device address of g_noalloc_gtab, per device
+}  // namespace
+
+extern "C" int mms_potential_direct_noalloc(const float *rho, float *phi, int xdim, int ydim, int zdim, double dx,
+                                            double dy, double dz, void *stream)
+{
+    if (!rho || !phi || xdim < 1 || ydim < 1 || zdim < 1 || !(dx > 0 && dy > 0 && dz > 0)) {
+        mms_set_error("mms_potential_direct_noalloc: bad argument");
+        return MMS_ERR_ARG;
+    }
+    const long long N = (long long)xdim * ydim * zdim;
+    if (N > MMS_NOALLOC_MAX_CELLS || xdim > MAX_X) {
+        mms_set_error("mms_potential_direct_noalloc: %d x %d x %d exceeds the fixed table of %lld cells "
+                      "(or xdim > %d)", xdim, ydim, zdim, MMS_NOALLOC_MAX_CELLS, MAX_X);
+        return MMS_ERR_ARG;
+    }
+    int dev = 0;
+    MMS_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        mms_set_error("mms_potential_direct_noalloc: device %d out of range", dev);
+        return MMS_ERR_ARG;
+    }
+    if (!g_noalloc_ptr[dev]) {
+        // one-time set-up on this device (the first call, with the device current)
+        float *p = nullptr;
+        MMS_CUDA_TRY(cudaGetSymbolAddress((void **)&p, g_noalloc_gtab));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)direct_smem_bytes(MAX_X)));
+        g_noalloc_ptr[dev] = p;
+    }
+    float *gtab = g_noalloc_ptr[dev];
+    GridK g;
+    g.X = xdim;
+    g.Y = ydim;
+    g.Z = zdim;
+    g.N = N;
+    g.dx = dx;
+    g.dy = dy;
+    g.dz = dz;
+    cudaStream_t st = (cudaStream_t)stream;
+    // every table entry the sum reads is rewritten here: nothing has to start at zero
+    k_build_gtab<<<div_up(N, 256), 256, 0, st>>>(gtab, g);
+    MMS_CUDA_TRY(cudaGetLastError());
+    dim3 grid((unsigned)(ydim * zdim), div_up(xdim, SEG));
+    k_direct<<<grid, DWARPS * 32, direct_smem_bytes(xdim), st>>>(rho, gtab, phi, g);
+    MMS_CUDA_TRY(cudaGetLastError());
+    return MMS_OK;
+}

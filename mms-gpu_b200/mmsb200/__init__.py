@@ -105,6 +105,7 @@ SIGNATURES = {
     "mms_march": (_I, [_VP, ctypes.POINTER(Controller), _D, _D, ctypes.POINTER(Record), _I, ctypes.POINTER(_I),
                        MARCH_CB, _VP]),
     "mms_diag_fma_tflops": (_I, [_I, ctypes.POINTER(_D)]),
+    "mms_potential_direct_noalloc": (_I, [_VP, _VP, _I, _I, _I, _D, _D, _D, _VP]),
     "mms_fmm_stage_times": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_D)]),
     "mms_fmm_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D),
                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
