@@ -176,9 +176,11 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
 int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double stage_flops[5],
                  long long *p2p_pairs, long long *m2l_pairs);
 
-/* Per-stage device time of the FMM potential (ms, mean over reps after one
- * warm-up): [0] P2M, [1] M2M, [2] M2L, [3] L2L, [4] L2P + P2P.  CUDA events on
- * ctx's stream between the stage launches; rho/phi are device arrays. */
+/* Per-stage device time of the FMM potential (ms per stage, all its levels):
+ * [0] P2M, [1] M2M, [2] M2L, [3] L2L, [4] L2P + P2P.  After one full
+ * evaluation each stage is re-launched `reps` times back to back between two
+ * CUDA events on ctx's stream (stages are idempotent on unchanged inputs);
+ * rho/phi are device arrays and phi ends up holding the potential of rho. */
 int mms_fmm_stage_times(mms_ctx *ctx, const float *rho, float *phi, int reps, double ms[5]);
 
 /* allocation-free exact potential -------------------------------------------- */

@@ -61,6 +61,9 @@ struct FmmPlan {
     float *Lpart = nullptr;   // [NSPLIT][boxes][NR] M2L partial locals
     int4 *m2l_items = nullptr;  // {level, parity, first target, 0}
     long long *lev_dev = nullptr;  // device copy of lev_off
+    float *near = nullptr;    // [N] near-field potential (P2P) before L2P adds the far field
+    cudaStream_t side = nullptr;   // P2P runs here, concurrently with P2M .. L2L
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     size_t bytes = 0;
     // algorithmic work per evaluation (for the roofline)
     double flops = 0;
@@ -445,22 +448,24 @@ __global__ void k_l2l_c(float *__restrict__ Lfin, const float *__restrict__ Lpar
     Lfin[b * f.NR + k] = v;
 }
 
-// Leaf kernel: L2P + exact P2P.  CTA = BB leaf boxes of one row; thread =
-// (box, target row y, layer z) holding the S targets of its row in registers.
-// For every source row of the 3x3 leaf neighbourhood the thread loads the 3S
+// Leaf kernels.  The near field (P2P) needs only the charges, so it runs on a
+// side stream concurrently with the far-field chain (P2M .. L2L); the L2P
+// kernel joins the two.
+//
+// k_p2p: exact near field.  CTA = BB leaf boxes of one row; thread = (box,
+// target row y, layer z) holding the S targets of its row in registers.  For
+// every source row of the 3x3 leaf neighbourhood the thread loads the 3S
 // charges and the 2S-entry near-field row G[|dz|][|dy|][.] into registers and
 // does 3S x S FMAs with compile-time indices |S + i - j|.
 template <int S, int BB>
-__global__ void __launch_bounds__(512) k_leaf(const float *__restrict__ rho, const float *__restrict__ Lleaf,
-                                               const float *__restrict__ Vt, const float *__restrict__ Gn,
-                                               float *__restrict__ phi, FmmDev f, int far)
+__global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, const float *__restrict__ Gn,
+                                              float *__restrict__ out, FmmDev f)
 {
     extern __shared__ __align__(16) float sl[];
     const int Z = f.Z;
     constexpr int W = (BB + 2) * S;        // charges per staged row
     float *qn = sl;                        // [Z][3S][W]
     float *g = qn + Z * 3 * S * W;         // [Z][2S][2S]
-    float *Lb = g + Z * 4 * S * S;         // [BB][NR]
     const int by = blockIdx.y, bx0 = blockIdx.x * BB;
     const int xs0 = bx0 * S - S, ys0 = by * S - S;
     for (int i = threadIdx.x; i < Z * 3 * S * W; i += blockDim.x) {
@@ -468,11 +473,6 @@ __global__ void __launch_bounds__(512) k_leaf(const float *__restrict__ rho, con
         qn[i] = (xx >= 0 && yy >= 0 && xx < f.X && yy < f.Y) ? rho[((long long)zz * f.Y + yy) * f.X + xx] : 0.f;
     }
     for (int i = threadIdx.x; i < Z * 4 * S * S; i += blockDim.x) g[i] = Gn[i];
-    if (far)
-        for (int i = threadIdx.x; i < BB * f.NR; i += blockDim.x) {
-            const int b = i / f.NR;
-            Lb[i] = (bx0 + b < f.nb) ? Lleaf[((long long)by * f.nb + bx0 + b) * f.NR + i % f.NR] : 0.f;
-        }
     __syncthreads();
     const int t = threadIdx.x;
     const int b = t / (S * Z), r = t % (S * Z);
@@ -513,34 +513,92 @@ __global__ void __launch_bounds__(512) k_leaf(const float *__restrict__ rho, con
                 }
         }
     }
-    if (far) {
-        const float *Lbb = Lb + b * f.NR;
-        const int c0 = lz * S * S + ly * S;
-        for (int k = 0; k < f.NR; k++) {
-            const float lk = Lbb[k];
-            const float *vrow = Vt + (long long)k * f.C + c0;
-            if constexpr (S % 4 == 0) {
-#pragma unroll
-                for (int v = 0; v < S / 4; v++) {
-                    const float4 u = __ldg(reinterpret_cast<const float4 *>(vrow) + v);
-                    acc[4 * v + 0] = fmaf(u.x, lk, acc[4 * v + 0]);
-                    acc[4 * v + 1] = fmaf(u.y, lk, acc[4 * v + 1]);
-                    acc[4 * v + 2] = fmaf(u.z, lk, acc[4 * v + 2]);
-                    acc[4 * v + 3] = fmaf(u.w, lk, acc[4 * v + 3]);
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < S; i++) acc[i] = fmaf(__ldg(&vrow[i]), lk, acc[i]);
-            }
-        }
-    }
     const int y = by * S + ly;
     if (bx0 + b >= f.nb || y >= f.Y) return;
 #pragma unroll
     for (int i = 0; i < S; i++) {
         const int x = (bx0 + b) * S + i;
-        if (x < f.X) phi[((long long)lz * f.Y + y) * f.X + x] = acc[i];
+        if (x < f.X) out[((long long)lz * f.Y + y) * f.X + x] = acc[i];
     }
+}
+
+// k_l2p: leaf locals (the leaf level's L2L: NSPLIT-summed M2L partials plus
+// the L2L of the parent's final local, none when the leaf level is 2), then
+// phi = near field + sum_k V[k][cell] L[k].  Same thread layout as k_p2p.
+template <int S, int BB>
+__global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, const float *__restrict__ Lpart_leaf,
+                                              const float *__restrict__ Lpar, const float *__restrict__ Tl2l,
+                                              const float *__restrict__ Vt, float *__restrict__ phi, FmmDev f,
+                                              long long part_stride, int nsplit)
+{
+    extern __shared__ __align__(16) float sl[];
+    const int Z = f.Z;
+    const int NE = f.NE, NO = f.NR - f.NE;
+    float *Ts = sl;                                   // L2L operator blocks
+    float *Lb = Ts + 4 * (NE * NE + NO * NO);         // [BB][NR] leaf locals
+    float *Lp = Lb + BB * f.NR;                       // [BB/2][NR] parent locals
+    const int by = blockIdx.y, bx0 = blockIdx.x * BB;
+    const int haspar = f.L > 2;
+    if (haspar) {
+        const int tsz = 4 * (NE * NE + NO * NO);
+        for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+            *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tl2l[i]));
+        const int np = f.nb >> 1;
+        for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
+            const int pb = (bx0 >> 1) + i / f.NR;
+            Lp[i] = (pb < np) ? Lpar[((long long)(by >> 1) * np + pb) * f.NR + i % f.NR] : 0.f;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < BB * f.NR; i += blockDim.x) {
+        const int b = i / f.NR, k = i % f.NR;
+        float v = 0.f;
+        if (bx0 + b < f.nb) {
+            const long long box = (long long)by * f.nb + bx0 + b;
+            if (haspar) {
+                const int c = ((bx0 + b) & 1) | ((by & 1) << 1);
+                const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+                const float *T = Ts + blk_base(c, NE, NO, blk);
+                const float *lp = Lp + (b >> 1) * f.NR + boff;
+                for (int j = 0; j < NB; j++) v = fmaf(T[j * NB + kk], lp[j], v);
+            }
+            for (int q = 0; q < nsplit; q++) v += Lpart_leaf[q * part_stride + box * f.NR + k];
+        }
+        Lb[i] = v;
+    }
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int b = t / (S * Z), r = t % (S * Z);
+    const int ly = r % S, lz = r / S;
+    const int y = by * S + ly;
+    if (bx0 + b >= f.nb || y >= f.Y) return;
+    const long long row = ((long long)lz * f.Y + y) * f.X + (long long)(bx0 + b) * S;
+    float acc[S];
+#pragma unroll
+    for (int i = 0; i < S; i++) acc[i] = ((bx0 + b) * S + i < f.X) ? near[row + i] : 0.f;
+    const float *Lbb = Lb + b * f.NR;
+    const int c0 = lz * S * S + ly * S;
+#pragma unroll 4
+    for (int k = 0; k < f.NR; k++) {
+        const float lk = Lbb[k];
+        const float *vrow = Vt + (long long)k * f.C + c0;
+        if constexpr (S % 4 == 0) {
+#pragma unroll
+            for (int v = 0; v < S / 4; v++) {
+                const float4 u = __ldg(reinterpret_cast<const float4 *>(vrow) + v);
+                acc[4 * v + 0] = fmaf(u.x, lk, acc[4 * v + 0]);
+                acc[4 * v + 1] = fmaf(u.y, lk, acc[4 * v + 1]);
+                acc[4 * v + 2] = fmaf(u.z, lk, acc[4 * v + 2]);
+                acc[4 * v + 3] = fmaf(u.w, lk, acc[4 * v + 3]);
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < S; i++) acc[i] = fmaf(__ldg(&vrow[i]), lk, acc[i]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < S; i++)
+        if ((bx0 + b) * S + i < f.X) phi[row + i] = acc[i];
 }
 
 __global__ void k_build_gn(float *__restrict__ Gn, int Z, int s, double dx, double dy, double dz)
@@ -581,48 +639,60 @@ int leaf_threads(const FmmDev &f)
     return t <= 512 ? t : 0;
 }
 
-size_t leaf_smem(const FmmDev &f)
+size_t p2p_smem(const FmmDev &f)
 {
     const int S = f.s, B = leaf_bb(S), W = (B + 2) * S;
-    return ((size_t)f.Z * 3 * S * W + (size_t)f.Z * 4 * S * S + (size_t)B * f.NR) * sizeof(float);
+    return ((size_t)f.Z * 3 * S * W + (size_t)f.Z * 4 * S * S) * sizeof(float);
 }
 
-int leaf_set_smem(int S, size_t bytes)
+size_t l2p_smem(const FmmDev &f)
 {
+    const int B = leaf_bb(f.s);
+    const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
+    return (tsz + (size_t)B * f.NR + (size_t)(B / 2) * f.NR) * sizeof(float);
+}
+
+#define MMS_LEAF_CASES(X) X(2, 8) X(4, 8) X(8, 4) X(16, 4)
+
+int leaf_set_smem(const FmmDev &f)
+{
+    const int a = (int)p2p_smem(f), b = (int)l2p_smem(f);
     cudaError_t e = cudaSuccess;
-    const int b = (int)bytes;
-    switch (S) {
-    case 2: e = cudaFuncSetAttribute(k_leaf<2, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
-    case 4: e = cudaFuncSetAttribute(k_leaf<4, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
-    case 8: e = cudaFuncSetAttribute(k_leaf<8, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
-    case 16: e = cudaFuncSetAttribute(k_leaf<16, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); break;
-    default: break;
+#define X(S_, B_)                                                                                  \
+    if (f.s == S_) {                                                                               \
+        if (a > 48 * 1024) e = cudaFuncSetAttribute(k_p2p<S_, B_>, cudaFuncAttributeMaxDynamicSharedMemorySize, a); \
+        if (e == cudaSuccess && b > 48 * 1024)                                                    \
+            e = cudaFuncSetAttribute(k_l2p<S_, B_>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); \
     }
+    MMS_LEAF_CASES(X)
+#undef X
     if (e != cudaSuccess) {
-        mms_set_error("leaf kernel shared memory (%zu B): %s", bytes, cudaGetErrorString(e));
+        mms_set_error("leaf kernel shared memory (%d / %d B): %s", a, b, cudaGetErrorString(e));
         return MMS_ERR_ARG;
     }
     return MMS_OK;
 }
 
-int leaf_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float *Lleaf, const float *Vt,
-                const float *Gn, float *phi, int far, cudaStream_t st)
+int p2p_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float *Gn, float *out, cudaStream_t st)
 {
-    const int t = leaf_threads(f);
-    const size_t sm = leaf_smem(f);
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
-    switch (f.s) {
-    case 2: k_leaf<2, 8><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
-    case 4: k_leaf<4, 8><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
-    case 8: k_leaf<8, 4><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
-    case 16: k_leaf<16, 4><<<grid, t, sm, st>>>(rho, Lleaf, Vt, Gn, phi, f, far); break;
-    default:
-        mms_set_error("no leaf kernel for side %d", f.s);
-        return MMS_ERR_ARG;
-    }
-    return MMS_OK;
+#define X(S_, B_) if (f.s == S_) { k_p2p<S_, B_><<<grid, leaf_threads(f), p2p_smem(f), st>>>(rho, Gn, out, f); return MMS_OK; }
+    MMS_LEAF_CASES(X)
+#undef X
+    mms_set_error("no leaf kernel for side %d", f.s);
+    return MMS_ERR_ARG;
 }
 
+int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float *Lpart_leaf, const float *Lpar,
+               const float *Tl2l, const float *Vt, float *phi, long long part_stride, int nsplit, cudaStream_t st)
+{
+    const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
+#define X(S_, B_) if (f.s == S_) { k_l2p<S_, B_><<<grid, leaf_threads(f), l2p_smem(f), st>>>(near, Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit); return MMS_OK; }
+    MMS_LEAF_CASES(X)
+#undef X
+    mms_set_error("no leaf kernel for side %d", f.s);
+    return MMS_ERR_ARG;
+}
 
 // resident-operator M2L specialisations: (NR, NE) for P = 1 .. 5
 #define MMS_M2L_RES_CASES(X) X(6, 4) X(12, 8) X(20, 12) X(30, 18) X(42, 24)
@@ -831,7 +901,16 @@ int fmm_plan_create(mms_ctx *ctx)
             mms_set_error("FMM plan: device allocation failed");
             return MMS_ERR_NOMEM;
         }
-        pl->bytes += (2 + NSPLIT) * ncoef * sizeof(float) + (size_t)Z * 4 * s * s * sizeof(float);
+        if (cudaMalloc((void **)&pl->near, (size_t)ctx->N * sizeof(float)) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&pl->side, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&pl->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&pl->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+            fmm_plan_destroy(ctx);
+            mms_set_error("FMM plan: stream/event/buffer creation failed");
+            return MMS_ERR_NOMEM;
+        }
+        pl->bytes += (2 + NSPLIT) * ncoef * sizeof(float) + (size_t)Z * 4 * s * s * sizeof(float) +
+                     (size_t)ctx->N * sizeof(float);
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Lpart, 0, NSPLIT * ncoef * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Mall, 0, ncoef * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Lall, 0, ncoef * sizeof(float), ctx->stream));
@@ -857,11 +936,9 @@ int fmm_plan_create(mms_ctx *ctx)
             MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2m_c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a1));
         if (a2 > 48 * 1024)
             MMS_CUDA_TRY(cudaFuncSetAttribute(k_l2l_c, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)a2));
+
     }
-    if (leaf_threads(f) > 0) {
-        const size_t lsm = leaf_smem(f);
-        if (lsm > 48 * 1024) MMS_TRY(leaf_set_smem(f.s, lsm));
-    }
+    if (leaf_threads(f) > 0) MMS_TRY(leaf_set_smem(f));
 
     // algorithmic work of one evaluation (FMA = 2 flops), per stage
     const long long nleafb = (long long)f.nb * f.nb;
@@ -914,22 +991,123 @@ void fmm_plan_destroy(mms_ctx *ctx)
     if (!pl) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Tm2lc, pl->Gn, pl->Mall, pl->Lall, pl->Lpart,
-                 pl->m2l_items, pl->lev_dev};
+                 pl->m2l_items, pl->lev_dev, pl->near};
     for (void *p : b)
         if (p) cudaFree(p);
+    if (pl->side) cudaStreamSynchronize(pl->side);
+    if (pl->ev_fork) cudaEventDestroy(pl->ev_fork);
+    if (pl->ev_join) cudaEventDestroy(pl->ev_join);
+    if (pl->side) cudaStreamDestroy(pl->side);
     delete pl;
     ctx->fmm = nullptr;
 }
 
 size_t fmm_plan_bytes(const mms_ctx *ctx) { return ctx->fmm ? ctx->fmm->bytes : 0; }
 
-// optional per-stage CUDA events (mms_fmm_stage_times): stage 0 P2M, 1 M2M,
-// 2 M2L, 3 L2L, 4 L2P+P2P; each mark records the end of that stage
-static thread_local cudaEvent_t *g_stage_ev = nullptr;
-
-static void stage_mark(mms_ctx *ctx, int stage)
+// L2P of the far field onto the near field already in pl->near
+static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
 {
-    if (g_stage_ev) cudaEventRecord(g_stage_ev[stage + 1], ctx->stream);
+    (void)rho;
+    FmmPlan *pl = ctx->fmm;
+    const FmmDev &f = pl->d;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    const int nsplit = pl->m2l_resident ? 1 : NSPLIT;
+    const float *Lpar = f.L > 2 ? pl->Lall + pl->lev_off[f.L - 1] * f.NR : nullptr;
+    MMS_TRY(l2p_launch(f, nbx, nby, pl->near, pl->Lpart + pl->lev_off[f.L] * f.NR, Lpar, pl->Tl2l, pl->Vt, phi,
+                       pl->nbox_total * f.NR, nsplit, ctx->stream));
+    MMS_LAUNCH_CHECK(ctx);
+    return MMS_OK;
+}
+
+// One stage of the FMM potential: 0 P2M, 1 M2M (all levels), 2 M2L (all
+// levels), 3 L2L (all levels, with the M2L partial sums), 4 L2P + P2P.  Every
+// stage only reads what earlier stages wrote, so re-running one stage on
+// unchanged inputs reproduces its output (mms_fmm_stage_times relies on that).
+static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *phi)
+{
+    FmmPlan *pl = ctx->fmm;
+    const FmmDev &f = pl->d;
+    const int far = f.L >= 2;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    const long long part_stride = pl->nbox_total * f.NR;
+    const int thr = ((f.NR + 31) / 32) * 32;
+    const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
+    const int KT = ((f.NR + 31) / 32) * 32;
+    const int nsplit = pl->m2l_resident ? 1 : NSPLIT;
+    if (stage < 4 && !far) return MMS_OK;
+    switch (stage) {
+    case 0: {
+        const long long leaf_off = pl->lev_off[f.L];
+        const int wsm = (f.C * f.NR) % 4 == 0 && (size_t)f.C * (BB + f.NR) * sizeof(float) <= 160 * 1024;
+        k_p2m_row<<<dim3(div_up(nbx, BB), nby), 128, (size_t)f.C * (BB + (wsm ? f.NR : 0)) * sizeof(float),
+                    ctx->stream>>>(rho, pl->Wt, pl->Mall + leaf_off * f.NR, f, wsm);
+        MMS_LAUNCH_CHECK(ctx);
+        break;
+    }
+    case 1:
+        for (int l = f.L - 1; l >= 2; l--) {
+            const int np = 1 << l;
+            k_m2m_c<<<np * np, 4 * KT, (tsz + 4 * (size_t)f.NR + 4 * (size_t)KT) * sizeof(float), ctx->stream>>>(
+                pl->Mall, pl->Tm2m, pl->lev_off[l], pl->lev_off[l + 1], np, f);
+            MMS_LAUNCH_CHECK(ctx);
+        }
+        break;
+    case 2: {
+        if (pl->m2l_resident) {
+            MMS_TRY(m2l_res_launch(f, pl->n_m2l_items, pl->Mall, pl->Lpart, pl->Tm2lc, pl->m2l_items, pl->lev_dev,
+                                   ctx->stream));
+        } else {
+            const int NBmax = std::max(f.NE, f.NR - f.NE);
+            const int KPmax = std::max(pl->KPb[0], pl->KPb[1]);
+            const size_t sm = ((size_t)NBmax * KPmax + 32 * (size_t)(NBmax | 1)) * sizeof(float);
+            k_m2l_split<<<dim3(pl->n_m2l_items, 2, NSPLIT), 32 * M2L_WARPS, sm, ctx->stream>>>(
+                pl->Mall, pl->Lpart, pl->Tm2l, pl->m2l_items, pl->lev_dev, f, pl->KPb[0], pl->KPb[1], NBmax,
+                part_stride);
+        }
+        MMS_LAUNCH_CHECK(ctx);
+        break;
+    }
+    case 3: {
+        // level 2 from its M2L partials, levels 3 .. L-1 one launch each; the
+        // leaf level is formed inside the leaf kernel (or by k_l2l_c for the
+        // generic leaf kernel)
+        const int lend = leaf_threads(f) > 0 ? f.L - 1 : f.L;
+        if (lend >= 2) {
+            k_l2l_c<<<16, thr, 0, ctx->stream>>>(pl->Lall, pl->Lpart, pl->Tl2l, 0, pl->lev_off[2], 4, 0,
+                                                 part_stride, nsplit, f);
+            MMS_LAUNCH_CHECK(ctx);
+        }
+        for (int l = 3; l <= lend; l++) {
+            const int nc = 1 << l, np = nc / 2;
+            k_l2l_c<<<np * np, 4 * KT, (tsz + (size_t)f.NR) * sizeof(float), ctx->stream>>>(
+                pl->Lall, pl->Lpart, pl->Tl2l, pl->lev_off[l - 1], pl->lev_off[l], nc, np, part_stride, nsplit, f);
+            MMS_LAUNCH_CHECK(ctx);
+        }
+        break;
+    }
+    case 4:
+        // (timing path) near field then far field, both on the main stream
+        if (leaf_threads(f) > 0) {
+            if (!far) {
+                MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, phi, ctx->stream));
+                MMS_LAUNCH_CHECK(ctx);
+            } else {
+                MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, ctx->stream));
+                MMS_LAUNCH_CHECK(ctx);
+                MMS_TRY(l2p_launch_far(ctx, rho, phi));
+            }
+        } else {
+            const size_t smem = ((size_t)f.Z * 9 * f.s * f.s + (size_t)f.Z * 4 * f.s * f.s + f.NR) * sizeof(float);
+            const int threads = ((f.C + 31) / 32) * 32;
+            k_l2p_p2p<<<f.nb * f.nb, threads, smem, ctx->stream>>>(rho, pl->Lall + pl->lev_off[f.L] * f.NR, pl->Vt,
+                                                                  pl->Gn, phi, f, far);
+            MMS_LAUNCH_CHECK(ctx);
+        }
+        break;
+    default:
+        break;
+    }
+    return MMS_OK;
 }
 
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
@@ -940,67 +1118,20 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
         return MMS_ERR_ARG;
     }
     const FmmDev &f = pl->d;
-    const int far = f.L >= 2;
+    if (leaf_threads(f) == 0 || f.L < 2) {
+        for (int st = 0; st < 5; st++) MMS_TRY(launch_fmm_stage(ctx, st, rho, phi));
+        return MMS_OK;
+    }
+    // fork: the near field on the side stream, the far-field chain on the main one
     const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
-    const bool tuned = leaf_threads(f) > 0;
-    const long long part_stride = pl->nbox_total * f.NR;
-    const int thr = ((f.NR + 31) / 32) * 32;
-    if (far) {
-        const long long leaf_off = pl->lev_off[f.L];
-        const int wsm = (f.C * f.NR) % 4 == 0 && (size_t)f.C * (BB + f.NR) * sizeof(float) <= 160 * 1024;
-        k_p2m_row<<<dim3(div_up(nbx, BB), nby), 128, (size_t)f.C * (BB + (wsm ? f.NR : 0)) * sizeof(float),
-                    ctx->stream>>>(rho, pl->Wt, pl->Mall + leaf_off * f.NR, f, wsm);
-        MMS_LAUNCH_CHECK(ctx);
-        stage_mark(ctx, 0);
-        const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
-        const int KT = ((f.NR + 31) / 32) * 32;
-        for (int l = f.L - 1; l >= 2; l--) {
-            const int np = 1 << l;
-            k_m2m_c<<<np * np, 4 * KT, (tsz + 4 * (size_t)f.NR + 4 * (size_t)KT) * sizeof(float), ctx->stream>>>(
-                pl->Mall, pl->Tm2m, pl->lev_off[l], pl->lev_off[l + 1], np, f);
-            MMS_LAUNCH_CHECK(ctx);
-            stage_mark(ctx, 1);
-        }
-        const int NBmax = std::max(f.NE, f.NR - f.NE);
-        const int KPmax = std::max(pl->KPb[0], pl->KPb[1]);
-        const size_t sm = ((size_t)NBmax * KPmax + 32 * (size_t)(NBmax | 1)) * sizeof(float);
-        int nsplit = NSPLIT;
-        if (pl->m2l_resident) {
-            MMS_TRY(m2l_res_launch(f, pl->n_m2l_items, pl->Mall, pl->Lpart, pl->Tm2lc, pl->m2l_items, pl->lev_dev,
-                                   ctx->stream));
-            nsplit = 1;
-        } else {
-            k_m2l_split<<<dim3(pl->n_m2l_items, 2, NSPLIT), 32 * M2L_WARPS, sm, ctx->stream>>>(
-                pl->Mall, pl->Lpart, pl->Tm2l, pl->m2l_items, pl->lev_dev, f, pl->KPb[0], pl->KPb[1], NBmax,
-                part_stride);
-        }
-        MMS_LAUNCH_CHECK(ctx);
-        stage_mark(ctx, 2);
-        k_l2l_c<<<16, thr, 0, ctx->stream>>>(pl->Lall, pl->Lpart, pl->Tl2l, 0, pl->lev_off[2], 4, 0, part_stride,
-                                             nsplit, f);
-        MMS_LAUNCH_CHECK(ctx);
-        for (int l = 3; l <= f.L; l++) {
-            const int nc = 1 << l, np = nc / 2;
-            k_l2l_c<<<np * np, 4 * KT, (tsz + (size_t)f.NR) * sizeof(float), ctx->stream>>>(
-                pl->Lall, pl->Lpart, pl->Tl2l, pl->lev_off[l - 1], pl->lev_off[l], nc, np, part_stride, nsplit, f);
-            MMS_LAUNCH_CHECK(ctx);
-        }
-        stage_mark(ctx, 3);
-    }
-    if (tuned) {
-        MMS_TRY(leaf_launch(f, nbx, nby, rho, pl->Lall + pl->lev_off[f.L] * f.NR, pl->Vt, pl->Gn, phi, far,
-                            ctx->stream));
-        MMS_LAUNCH_CHECK(ctx);
-        stage_mark(ctx, 4);
-    } else {
-        const size_t smem = ((size_t)f.Z * 9 * f.s * f.s + (size_t)f.Z * 4 * f.s * f.s + f.NR) * sizeof(float);
-        const int threads = ((f.C + 31) / 32) * 32;
-        k_l2p_p2p<<<f.nb * f.nb, threads, smem, ctx->stream>>>(rho, pl->Lall + pl->lev_off[f.L] * f.NR, pl->Vt,
-                                                              pl->Gn, phi, f, far);
-        MMS_LAUNCH_CHECK(ctx);
-        stage_mark(ctx, 4);
-    }
-    return MMS_OK;
+    MMS_CUDA_TRY(cudaEventRecord(pl->ev_fork, ctx->stream));
+    MMS_CUDA_TRY(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
+    MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, pl->side));
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
+    for (int st = 0; st < 4; st++) MMS_TRY(launch_fmm_stage(ctx, st, rho, phi));
+    MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
+    return l2p_launch_far(ctx, rho, phi);
 }
 
 int fmm_default_leaf(int P, int X, int Y)
@@ -1035,26 +1166,21 @@ extern "C" int mms_fmm_stage_times(mms_ctx *ctx, const float *rho, float *phi, i
         mms_set_error("mms_fmm_stage_times: bad argument or no FMM plan");
         return MMS_ERR_ARG;
     }
-    cudaEvent_t ev[6];
-    for (int i = 0; i < 6; i++) MMS_CUDA_TRY(cudaEventCreate(&ev[i]));
-    for (int i = 0; i < 5; i++) ms[i] = 0.0;
-    int st = launch_potential_fmm(ctx, rho, phi);  // warm-up
-    for (int r = 0; r < reps && st == MMS_OK; r++) {
-        cudaEventRecord(ev[0], ctx->stream);
-        for (int i = 1; i < 6; i++) cudaEventRecord(ev[i], ctx->stream);  // stages that do not run keep 0 width
-        g_stage_ev = ev;
-        st = launch_potential_fmm(ctx, rho, phi);
-        g_stage_ev = nullptr;
-        cudaEventSynchronize(ev[5]);
-        float prev = 0.f;
-        for (int i = 1; i < 6; i++) {
-            float t = 0.f;
-            cudaEventElapsedTime(&t, ev[0], ev[i]);
-            if (t < prev) t = prev;
-            ms[i - 1] += (t - prev) / reps;
-            prev = t;
-        }
+    cudaEvent_t e0, e1;
+    MMS_CUDA_TRY(cudaEventCreate(&e0));
+    MMS_CUDA_TRY(cudaEventCreate(&e1));
+    int st = launch_potential_fmm(ctx, rho, phi);  // valid inputs for every stage
+    for (int s = 0; s < 5 && st == MMS_OK; s++) {
+        st = launch_fmm_stage(ctx, s, rho, phi);  // warm
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < reps && st == MMS_OK; r++) st = launch_fmm_stage(ctx, s, rho, phi);
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms[s] = (double)t / reps;
     }
-    for (int i = 0; i < 6; i++) cudaEventDestroy(ev[i]);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     return st;
 }
