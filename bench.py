@@ -372,18 +372,20 @@ def run_ours(args):
 
 
 STAGE_KERNEL = {"p2m": "k_p2m_row", "m2m": "k_m2m_c (one launch per level)", "m2l": "k_m2l_res / k_m2l_split",
-                "l2l": "k_l2l_c (one launch per level)", "l2p_p2p": "k_leaf"}
+                "l2l": "k_l2l_c (one launch per level)", "l2p_p2p": "k_p2p + k_l2p"}
 
 
 def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):
-    """FMM roofline: every stage is FP32-pipe work (SIMT).  Each stage is timed
-    live with CUDA events over back-to-back re-launches on the library's
-    stream; the dominant stage's algorithmic flops over its time, against the
-    measured FP32 FMA peak."""
+    """FMM roofline for its largest single kernel, the M2L (one launch per
+    evaluation, all levels; the largest share of the ncu launch list).  Each
+    stage is timed live with CUDA events over back-to-back re-launches on the
+    library's stream; achieved = the M2L's algorithmic flops (NE^2 + NO^2
+    multiply-adds per interaction-list box pair) over its time, against the
+    measured FP32 FMA peak.  All stage times and flops are reported beside it."""
     import mmsb200
     st = mmsb200.fmm_stats(ctx)
     times = mmsb200.fmm_stage_times(ctx, rho, phi, reps=20)
-    dom = max(times, key=times.get)
+    dom = "m2l"
     roof = {"kernel": f"{STAGE_KERNEL[dom]} (FMM stage {dom})", "bound": "fp32", "peak": fma_peak,
             "unit": "TFLOP/s",
             "peak_source": "measured FP32 FMA microbenchmark (mms_diag_fma_tflops), of measured"}
