@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--dt", type=float, default=1e-13)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["single", "ensemble"], default="single",
+                    help="single: the 256x256x3 metric; ensemble: the batched-ensemble configuration")
+    ap.add_argument("--ensemble-size", type=int, default=512)
     return ap.parse_args()
 
 
@@ -399,10 +402,68 @@ def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):
     return roof
 
 
+def run_ensemble(args):
+    """Batched ensemble: `--ensemble-size` independent simulations (sides 16..64
+    in steps of 8, x3 layers, rectangle/disc/ellipse masks, random M, random
+    in-plane |B| <= 50 mT; dt = 1e-13 s), one CUDA graph per ensemble step.
+    Under torchrun the instances are partitioned over ranks by cost with no
+    collective on the data path; value = ensemble steps/s of the whole job."""
+    import torch
+    import mmsb200
+    from mmsb200 import geometry
+    from mmsb200.ensemble import Ensemble, cost, partition
+    ws, rank, local = dist_init()
+    dims, masks, Ms, bext = geometry.ensemble_instances(args.ensemble_size, seed=2010)
+    mine = partition([cost(d) for d in dims], ws, rank)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ens = Ensemble([dims[i] for i in mine], (5e-9, 5e-9, 5e-9), mmsb200.make_params(external=True),
+                   bext=[bext[i] for i in mine], stream=stream.cuda_stream)
+    ens.state_set([masks[i] for i in mine], [Ms[i] for i in mine])
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ens.run_fixed(args.dt, max(args.warmup, 3), use_graph=True)
+    ens.sync()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = ens.kernel_launches
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        ens.run_fixed(args.dt, 1, use_graph=True)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    launches = ens.kernel_launches - l0
+    barrier(ws)
+    clk = clocks.stop()
+    ms_total = max_over_ranks(ws, float(sum(a.elapsed_time(b) for a, b in ev)))
+    cells = sum(X * Y * Z for X, Y, Z in dims)
+    ens.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    value = args.steps / (ms_total * 1e-3)
+    print(json.dumps({"metric": f"ensemble LLG RK4 steps/s ({args.ensemble_size} instances, 16..64 x 16..64 x 3)",
+                      "value": value, "unit": "ensemble steps/s", "n_gpus": ws, "steps": args.steps,
+                      "warmup": max(args.warmup, 3), "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+                      "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+                      "config": {"workload": "ensemble_rk4", "instances": args.ensemble_size, "cells": cells,
+                                 "solver": "direct (batched)", "dt_s": args.dt,
+                                 "l2": "flushed between timed steps", "parallelism": f"instance partition x{ws}"},
+                      "cell_steps_per_s": value * cells, "gpu_launches": int(launches), "clocks": clk}))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "ensemble":
+        return run_ensemble(args)
     return run_ours(args)
 
 

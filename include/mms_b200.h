@@ -183,6 +183,33 @@ int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double 
  * rho/phi are device arrays and phi ends up holding the potential of rho. */
 int mms_fmm_stage_times(mms_ctx *ctx, const float *rho, float *phi, int reps, double ms[5]);
 
+/* batched ensemble ----------------------------------------------------------- */
+/* Many independent simulations of uneven grid size (same cell size and
+ * material) advance together: one kernel launch per RK4 stage for the whole
+ * ensemble, driven by an instance offset table; exact direct-sum demag per
+ * instance; one CUDA graph per step.  Each instance has its own constant
+ * external field bext (T), applied when params->external != 0.  No reference
+ * counterpart (the reference runs one simulation per process). */
+typedef struct {
+    int xdim, ydim, zdim;    /* 1 <= xdim <= 256                               */
+    double bext[3];          /* constant external field (T)                    */
+} mms_ens_instance;
+
+typedef struct mms_ens mms_ens;
+
+int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, double dz,
+                   const mms_params *params, void *stream, mms_ens **out);
+int mms_ens_destroy(mms_ens *ens);
+/* total cells (sum over instances) */
+long long mms_ens_cells(const mms_ens *ens);
+int64_t mms_ens_kernel_launches(const mms_ens *ens);
+/* material (u8) and M (FP64 AoS) of all instances concatenated in instance
+ * order, each in the cell order z*Y*X + y*X + x; host pointers */
+int mms_ens_state_set(mms_ens *ens, const uint8_t *material, const double *M);
+int mms_ens_state_get(mms_ens *ens, double *M, double *t);
+int mms_ens_run_fixed(mms_ens *ens, double dt, int nsteps, int use_graph);
+int mms_ens_sync(mms_ens *ens);
+
 /* allocation-free exact potential -------------------------------------------- */
 /* No counterpart in the reference.  The exact direct-sum potential for callers
  * that cannot allocate device memory (a host whose pool allocator owns the

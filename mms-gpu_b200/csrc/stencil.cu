@@ -16,17 +16,13 @@
 
 #include <math.h>
 
+#include "stencil_dev.cuh"
+
 namespace {
 
-constexpr int TPB = 256;
+using namespace mmsdev;
 
-__device__ __forceinline__ void cell_xyz(long long i, const GridK &g, int &x, int &y, int &z)
-{
-    x = (int)(i % g.X);
-    long long r = i / g.X;
-    y = (int)(r % g.Y);
-    z = (int)(r / g.Y);
-}
+constexpr int TPB = 256;
 
 // ---- FP32 AoS, reference operation order ---------------------------------
 
@@ -161,86 +157,6 @@ __global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho,
     double z2 = (z != g.Z - 1) ? Mz[i + sz] : 0.0;
     double z0 = (z != 0) ? Mz[i - sz] : 0.0;
     rho[i] = (float)(0.5 * ((x2 - x0) / g.dx + (y2 - y0) / g.dy + (z2 - z0) / g.dz));
-}
-
-// clamped piecewise-linear B(t) table, or the reference's ramp (ode_functions.cpp:61)
-__device__ __forceinline__ void hext_at(const PhysK &p, const double *__restrict__ tab, double t, double H[3])
-{
-    H[0] = H[1] = H[2] = 0.0;
-    if (!p.external) return;
-    if (p.n_hext == 0) {
-        H[0] = (1.0 / p.mu0) * ((t < 1e-9) ? (-0.3 / 1e-9 * t + 0.3) : 0.0);
-        return;
-    }
-    const int n = p.n_hext;
-    double b0, b1, b2;
-    if (t <= tab[0]) {
-        b0 = tab[1]; b1 = tab[2]; b2 = tab[3];
-    } else if (t >= tab[4 * (n - 1)]) {
-        b0 = tab[4 * (n - 1) + 1]; b1 = tab[4 * (n - 1) + 2]; b2 = tab[4 * (n - 1) + 3];
-    } else {
-        int k = 0;
-        while (k + 1 < n && tab[4 * (k + 1)] < t) k++;
-        const double w = (t - tab[4 * k]) / (tab[4 * (k + 1)] - tab[4 * k]);
-        b0 = (1 - w) * tab[4 * k + 1] + w * tab[4 * (k + 1) + 1];
-        b1 = (1 - w) * tab[4 * k + 2] + w * tab[4 * (k + 1) + 2];
-        b2 = (1 - w) * tab[4 * k + 3] + w * tab[4 * (k + 1) + 3];
-    }
-    H[0] = b0 / p.mu0;
-    H[1] = b1 / p.mu0;
-    H[2] = b2 / p.mu0;
-}
-
-// effective field at cell i from phi (FP32) and the FP64 stage state
-__device__ __forceinline__ void field_soa(const float *__restrict__ phi, const double *__restrict__ M, long long i,
-                                          int x, int y, int z, const GridK &g, const PhysK &p, const double he[3],
-                                          double H[3])
-{
-    const long long sy = g.X, sz = (long long)g.X * g.Y;
-    H[0] = he[0];
-    H[1] = he[1];
-    H[2] = he[2];
-    if (p.demag) {
-        double x2 = (x != g.X - 1) ? (double)phi[i + 1] : 0.0;
-        double x0 = (x != 0) ? (double)phi[i - 1] : 0.0;
-        double y2 = (y != g.Y - 1) ? (double)phi[i + sy] : 0.0;
-        double y0 = (y != 0) ? (double)phi[i - sy] : 0.0;
-        double z2 = (z != g.Z - 1) ? (double)phi[i + sz] : 0.0;
-        double z0 = (z != 0) ? (double)phi[i - sz] : 0.0;
-        H[0] += p.cdemag * (x2 - x0) / (2 * g.dx);
-        H[1] += p.cdemag * (y2 - y0) / (2 * g.dy);
-        H[2] += p.cdemag * (z2 - z0) / (2 * g.dz);
-    }
-    if (p.exchange) {
-        const double idx2 = 1.0 / (g.dx * g.dx), idy2 = 1.0 / (g.dy * g.dy), idz2 = 1.0 / (g.dz * g.dz);
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const double *Mc = M + c * g.N;
-            double m0 = Mc[i];
-            double xp = (x != g.X - 1) ? Mc[i + 1] : 0.0;
-            double xm = (x != 0) ? Mc[i - 1] : 0.0;
-            double yp = (y != g.Y - 1) ? Mc[i + sy] : 0.0;
-            double ym = (y != 0) ? Mc[i - sy] : 0.0;
-            double zp = (z != g.Z - 1) ? Mc[i + sz] : 0.0;
-            double zm = (z != 0) ? Mc[i - sz] : 0.0;
-            H[c] += p.cexch * ((xp + xm - 2 * m0) * idx2 + (yp + ym - 2 * m0) * idy2 + (zp + zm - 2 * m0) * idz2);
-        }
-    }
-}
-
-// ode_functions.cpp:11-18
-__device__ __forceinline__ void llg(const double m[3], const double h[3], const PhysK &p, double k[3])
-{
-    const double cx = m[1] * h[2] - m[2] * h[1];
-    const double cy = m[2] * h[0] - m[0] * h[2];
-    const double cz = m[0] * h[1] - m[1] * h[0];
-    const double ex = m[1] * cz - m[2] * cy;
-    const double ey = m[2] * cx - m[0] * cz;
-    const double ez = m[0] * cy - m[1] * cx;
-    const double a = p.alpha * p.gamma / p.Ms;
-    k[0] = -p.gamma * cx - a * ex;
-    k[1] = -p.gamma * cy - a * ey;
-    k[2] = -p.gamma * cz - a * ez;
 }
 
 // One RK4 stage (ode_functions.cpp:96-145):

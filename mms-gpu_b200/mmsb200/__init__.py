@@ -106,6 +106,14 @@ SIGNATURES = {
                        MARCH_CB, _VP]),
     "mms_diag_fma_tflops": (_I, [_I, ctypes.POINTER(_D)]),
     "mms_potential_direct_noalloc": (_I, [_VP, _VP, _I, _I, _I, _D, _D, _D, _VP]),
+    "mms_ens_create": (_I, [_VP, _I, _D, _D, _D, ctypes.POINTER(Params), _VP, ctypes.POINTER(_VP)]),
+    "mms_ens_destroy": (_I, [_VP]),
+    "mms_ens_cells": (ctypes.c_longlong, [_VP]),
+    "mms_ens_kernel_launches": (_I64, [_VP]),
+    "mms_ens_state_set": (_I, [_VP, _VP, _VP]),
+    "mms_ens_state_get": (_I, [_VP, _VP, ctypes.POINTER(_D)]),
+    "mms_ens_run_fixed": (_I, [_VP, _D, _I, _I]),
+    "mms_ens_sync": (_I, [_VP]),
     "mms_fmm_stage_times": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_D)]),
     "mms_fmm_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D),
                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),

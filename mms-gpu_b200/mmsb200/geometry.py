@@ -156,3 +156,30 @@ def per_dot_random_inplane(X, Y, Z, r, pitch, seed, Ms=MS_PERMALLOY):
             ph = g.uniform(0, 2 * np.pi)
             M[dot != 0] = [np.cos(ph), np.sin(ph), 0.0]
     return mask, M * Ms
+
+
+def ensemble_instances(n, seed=2010, sides=(16, 24, 32, 40, 48, 56, 64), Z=3, bmax=0.05):
+    """The batched-ensemble workload: instance i (seed + i) gets sides drawn
+    uniformly from `sides`, a rectangle, disc or ellipse mask (material in the
+    middle layers), random M on the sphere and a random in-plane constant
+    external field with |B| <= bmax tesla.  Returns (dims, masks, Ms, bext)."""
+    dims, masks, Ms, bext = [], [], [], []
+    for i in range(n):
+        g = rng(seed + i)
+        X = int(g.choice(sides))
+        Y = int(g.choice(sides))
+        kind = int(g.integers(0, 3))
+        if kind == 0:
+            mask = rectangle(X, Y, Z)
+        elif kind == 1:
+            mask = disc(X, Y, Z, (min(X, Y) - 2) / 2)
+        else:
+            mask = from_plane(ellipse_plane(X, Y, (X - 1) / 2, (Y - 1) / 2, (X - 2) / 2, (Y - 2) / 3), Z)
+        M = random_sphere(mask, seed + 100000 + i)
+        b = bmax * np.sqrt(g.uniform(0, 1))
+        ph = g.uniform(0, 2 * np.pi)
+        dims.append((X, Y, Z))
+        masks.append(mask)
+        Ms.append(M)
+        bext.append((b * np.cos(ph), b * np.sin(ph), 0.0))
+    return dims, masks, Ms, bext
