@@ -229,6 +229,13 @@ int mms_potential_direct_noalloc(const float *rho, float *phi, int xdim, int ydi
                                  double dx, double dy, double dz, void *stream);
 
 /* diagnostics ---------------------------------------------------------------- */
+/* The library's tcgen05 tensor-core GEMM on BF16 operands: C = A B^T (beta 0)
+ * or C += A B^T (beta 1); A M x K and B N x K row-major (K contiguous), C
+ * M x N FP32 row-major; K, lda, ldb multiples of 8; bn = 64 or 128 (tile N).
+ * Device pointers; synchronises `stream`.  No reference counterpart (used to
+ * validate the core behind the tensor-core M2L and the surrogate). */
+int mms_diag_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C, int ldc,
+                       int M, int N, int K, int beta, int bn, void *stream);
 /* FP32 FMA throughput of the current device in TFLOP/s (a microbenchmark of
  * `reps` launches, one wave of 8 CTAs per SM): the roofline denominator of the
  * FP32-pipe-bound kernels (direct sum, near field).  No reference counterpart. */

@@ -137,6 +137,11 @@ void fmm_plan_destroy(mms_ctx *ctx);
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi);
 size_t fmm_plan_bytes(const mms_ctx *ctx);
 
+// tcgen05 BF16 GEMM (gemm.cu): C (+)= A B^T, A M x K, B N x K, K-major
+int umma_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C, int ldc, int M, int N, int K, int beta,
+                   int bn, cudaStream_t st);
+int umma_check_error();
+
 // potential with the context's solver
 int launch_potential(mms_ctx *ctx, const float *rho, float *phi);
 

@@ -105,6 +105,7 @@ SIGNATURES = {
     "mms_march": (_I, [_VP, ctypes.POINTER(Controller), _D, _D, ctypes.POINTER(Record), _I, ctypes.POINTER(_I),
                        MARCH_CB, _VP]),
     "mms_diag_fma_tflops": (_I, [_I, ctypes.POINTER(_D)]),
+    "mms_diag_gemm_bf16": (_I, [_VP, _I, _VP, _I, _VP, _I, _I, _I, _I, _I, _I, _VP]),
     "mms_potential_direct_noalloc": (_I, [_VP, _VP, _I, _I, _I, _D, _D, _D, _VP]),
     "mms_ens_create": (_I, [_VP, _I, _D, _D, _D, ctypes.POINTER(Params), _VP, ctypes.POINTER(_VP)]),
     "mms_ens_destroy": (_I, [_VP]),
