@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--solver", choices=["fmm", "direct"], default=os.environ.get("MMS_BENCH_SOLVER", "fmm"))
     ap.add_argument("--order", type=int, default=4, help="FMM expansion order P")
     ap.add_argument("--leaf", type=int, default=0, help="FMM leaf side in cells (0 = autotuned)")
+    ap.add_argument("--m2l", type=int, default=int(os.environ.get("MMS_BENCH_M2L", "0")),
+                    help="FMM M2L: 0 auto, 1 FP32 SIMT, 2 tensor cores (split BF16)")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--dt", type=float, default=1e-13)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -231,7 +233,7 @@ def run_ours(args):
     grid = mmsb200.Grid(X, Y, Z, *d)
     params = mmsb200.make_params(external=True, hext_t=hext_t, hext_b=hext_b)
     kind = mmsb200.SOLVER_FMM if args.solver == "fmm" else mmsb200.SOLVER_DIRECT
-    solver = mmsb200.make_solver(kind, args.order, args.leaf)
+    solver = mmsb200.make_solver(kind, args.order, args.leaf, args.m2l)
     # a dedicated stream: the library's kernels and every timing event live on it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -361,7 +363,8 @@ def run_ours(args):
            f"({L2_FLUSH_BYTES >> 20} MB write, outside the timed events)", "graph": "one CUDA graph per RK4 step",
            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
     if args.solver == "fmm":
-        cfg.update({"P": args.order, "leaf": args.leaf or "auto"})
+        cfg.update({"P": args.order, "leaf": args.leaf or "auto",
+                    "m2l": {0: "auto", 1: "fp32 simt", 2: "tensor cores (split bf16)"}[args.m2l]})
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": cfg,

@@ -84,7 +84,9 @@ typedef struct {
     int kind;                /* mms_solver_kind                                */
     int fmm_order;           /* expansion order P (FMM), 1..9                  */
     int fmm_leaf;            /* leaf box side in cells (FMM), 2..16, or 0=auto */
-    int reserved[5];
+    int m2l_mode;            /* FMM M2L: 0 auto, 1 FP32 SIMT, 2 tensor cores
+                                (tcgen05, split-BF16 hi/lo products)          */
+    int reserved[4];
 } mms_solver;
 
 typedef struct mms_ctx mms_ctx;

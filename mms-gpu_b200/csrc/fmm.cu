@@ -25,8 +25,11 @@
 #include <algorithm>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "fmm_ops.hpp"
 #include "mms_internal.cuh"
+#include "umma.cuh"
 
 namespace {
 
@@ -38,6 +41,17 @@ struct FmmDev {
     int X, Y;
     float inv_w;              // 1 / leaf width (m): L2P scale
 };
+
+// one GEMM of the grouped tensor-core M2L (a parity class x a parity block)
+struct TcGroup {
+    const __nv_bfloat16 *A;
+    const __nv_bfloat16 *B;
+    float *C;
+    const int *rowmap;
+    int lda, ldb, ldc, M, N, K;
+    int pad[2];
+};
+
 
 }  // namespace
 
@@ -55,6 +69,20 @@ struct FmmPlan {
     float *Tm2l = nullptr;    // [49][2][NBmax(j)][KP(k)] parity blocks, k padded
     float *Tm2lc = nullptr;   // [49][even NE x NE | odd NO x NO] compact, j-major (low orders)
     int m2l_resident = 0;     // 1: k_m2l_res (all operators in shared memory)
+    int m2l_tc = 0;           // 1: tensor-core M2L (gather + grouped tcgen05 GEMM)
+    // tensor-core M2L: per parity block b, A'_b rows = every box of levels >= 2
+    // grouped by parity class, each row [S_hi | S_hi | S_lo] over the class's
+    // 27 offsets; B'_{p,b} = [T_hi | T_lo | T_hi] operator rows
+    int tcK[2] = {0, 0};      // 27 * NB padded to 8, per block
+    int tcNBp[2] = {0, 0};
+    int tc_rows = 0;
+    __nv_bfloat16 *tcA[2] = {nullptr, nullptr};
+    __nv_bfloat16 *tcB = nullptr;   // [4 parities][2 blocks] regions
+    int *tc_rowmap = nullptr;       // row -> box index (all levels)
+    int4 *tc_rowinfo = nullptr;     // row -> {level, parity, target in class}
+    TcGroup *tc_groups = nullptr;   // [8] on the device
+    std::vector<TcGroup> tc_group_host;
+    int tc_maxm = 0;
     float *Gn = nullptr;      // [Z][2s][2s] near-field dV/|r|
     float *Mall = nullptr;    // [boxes of all levels][NR]
     float *Lall = nullptr;    // final locals
@@ -601,6 +629,64 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
         if ((bx0 + b) * S + i < f.X) phi[row + i] = acc[i];
 }
 
+// ---- tensor-core M2L ------------------------------------------------------
+// Gather: row r (a target box of one parity class at one level) of A'_b gets,
+// for each of the class's 27 offsets q, the source multipole block b
+// (NB floats, zero when the source is off the grid) split into BF16 hi and
+// lo, laid out [hi | hi | lo] over K = 3 * 27 * NBp.  A grouped tcgen05 GEMM
+// then forms sum_q S_q T_q^T from hi*hi + hi*lo + lo*hi in one K sweep
+// (relative error ~2^-16 of each product: the split recovers far more than
+// BF16 alone, below the FMM truncation error for P <= 6).
+__global__ void k_m2l_gather(const float *__restrict__ Mall, __nv_bfloat16 *__restrict__ A0,
+                             __nv_bfloat16 *__restrict__ A1, const int4 *__restrict__ rowinfo,
+                             const long long *__restrict__ lev_off, FmmDev f, int K0, int K1, int NBp0, int NBp1)
+{
+    const int r = blockIdx.x, blk = blockIdx.y;
+    const int4 ri = rowinfo[r];
+    const int lev = ri.x, px = ri.y & 1, py = ri.y >> 1, t = ri.z;
+    const int n = 1 << lev, nh = n >> 1;
+    const int tx = 2 * (t % nh) + px, ty = 2 * (t / nh) + py;
+    const int NB = blk ? f.NR - f.NE : f.NE, NBp = blk ? NBp1 : NBp0, K = blk ? K1 : K0;
+    const int boff = blk ? f.NE : 0;
+    __nv_bfloat16 *row = (blk ? A1 : A0) + (long long)r * 3 * K;
+    const long long off = lev_off[lev];
+    for (int e = threadIdx.x; e < 27 * NBp; e += blockDim.x) {
+        const int q = e / NBp, j = e % NBp;
+        // offset q of the class, in the order the operators were packed
+        const int oyi = q / 6, oxi = q % 6;  // 6 x 6 minus the 3 x 3 near block, skipping it
+        int cnt = 0, ox = 0, oy = 0;
+        for (int yy = 0; yy < 6; yy++)
+            for (int xx = 0; xx < 6; xx++) {
+                const int dx = px - 3 + xx, dy = py - 3 + yy;
+                if (max(abs(dx), abs(dy)) < 2) continue;
+                if (cnt == q) { ox = dx; oy = dy; }
+                cnt++;
+            }
+        (void)oyi; (void)oxi;
+        float v = 0.f;
+        const int sx = tx - ox, sy = ty - oy;
+        if (j < NB && sx >= 0 && sy >= 0 && sx < n && sy < n) v = Mall[(off + (long long)sy * n + sx) * f.NR + boff + j];
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        row[q * NBp + j] = hi;
+        row[K + q * NBp + j] = hi;
+        row[2 * K + q * NBp + j] = lo;
+    }
+}
+
+__device__ int g_m2l_tc_err;
+
+__global__ void __launch_bounds__(128) k_m2l_gemm(const TcGroup *__restrict__ groups)
+{
+    extern __shared__ uint8_t raw[];
+    const TcGroup g = groups[blockIdx.z];
+    const int m0 = blockIdx.x * umma::BM;
+    if (m0 >= g.M) return;  // before any tensor-memory allocation
+    uint8_t *base = (uint8_t *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+    umma::Smem<64> &s = *reinterpret_cast<umma::Smem<64> *>(base);
+    umma::gemm_tile<64>(g.A, g.lda, g.B, g.ldb, g.C, g.ldc, g.M, g.N, g.K, m0, 0, 0, &g_m2l_tc_err, s, g.rowmap);
+}
+
 __global__ void k_build_gn(float *__restrict__ Gn, int Z, int s, double dx, double dy, double dz)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -851,7 +937,50 @@ int fmm_plan_create(mms_ctx *ctx)
             for (int j = 0; j < NB; j++)
                 for (int k = 0; k < NB; k++) dst[(size_t)j * NB + k] = src[(size_t)j * KP + k];
         }
-    pl->m2l_resident = m2l_res_supported(NR, f.NE);
+    const int m2l_mode = ctx->s.m2l_mode;
+    // auto: the FP32 SIMT kernels; at 256x256x3 the tensor-core path measured
+    // slower (materialised gather + a latency-bound 2-stage K loop over few CTAs)
+    pl->m2l_tc = (m2l_mode == 2);
+    pl->m2l_resident = !pl->m2l_tc && m2l_res_supported(NR, f.NE);
+    // tensor-core M2L operands: B'_{p,b} rows k = [T_hi | T_lo | T_hi] over the
+    // class's 27 offsets (q-major, NBp-padded), matching k_m2l_gather's order
+    std::vector<__nv_bfloat16> tcB;
+    std::vector<long long> tcBoff(8, 0);
+    if (pl->m2l_tc) {
+        for (int blk = 0; blk < 2; blk++) {
+            const int NB = blk ? NB1 : NB0;
+            pl->tcNBp[blk] = (NB + 7) & ~7;
+            pl->tcK[blk] = 27 * pl->tcNBp[blk];
+        }
+        for (int par = 0; par < 4; par++) {
+            const int px = par & 1, py = par >> 1;
+            for (int blk = 0; blk < 2; blk++) {
+                const int NB = blk ? NB1 : NB0, NBp = pl->tcNBp[blk], K = pl->tcK[blk], KP = pl->KPb[blk];
+                tcBoff[par * 2 + blk] = (long long)tcB.size();
+                std::vector<__nv_bfloat16> Bg((size_t)NB * 3 * K, __float2bfloat16_rn(0.f));
+                int q = 0;
+                for (int yy = 0; yy < 6; yy++)
+                    for (int xx = 0; xx < 6; xx++) {
+                        const int ox = px - 3 + xx, oy = py - 3 + yy;
+                        if (std::max(abs(ox), abs(oy)) < 2) continue;
+                        const int o = (oy + 3) * 7 + (ox + 3);
+                        const float *src = &Tm2l[((size_t)o * 2 + blk) * NBmax * KPmax];
+                        for (int k = 0; k < NB; k++)
+                            for (int j = 0; j < NB; j++) {
+                                const float v = src[(size_t)j * KP + k];
+                                const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+                                const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+                                const size_t base = (size_t)k * 3 * K + (size_t)q * NBp + j;
+                                Bg[base] = hi;
+                                Bg[base + K] = lo;
+                                Bg[base + 2 * K] = hi;
+                            }
+                        q++;
+                    }
+                tcB.insert(tcB.end(), Bg.begin(), Bg.end());
+            }
+        }
+    }
     if (max_offblock > 1e-9) {
         delete pl;
         ctx->fmm = nullptr;
@@ -875,6 +1004,27 @@ int fmm_plan_create(mms_ctx *ctx)
     }
     pl->n_m2l_items = (int)items.size();
 
+    // tensor-core M2L rows: every box of levels >= 2, grouped by parity class
+    std::vector<int> tc_rowmap;
+    std::vector<int4> tc_rowinfo;
+    int tc_base[5] = {0, 0, 0, 0, 0};
+    if (pl->m2l_tc) {
+        for (int par = 0; par < 4; par++) {
+            tc_base[par] = (int)tc_rowmap.size();
+            for (int l = 2; l <= f.L; l++) {
+                const int nh = (1 << l) / 2;
+                for (int t = 0; t < nh * nh; t++) {
+                    const int bx = 2 * (t % nh) + (par & 1), by = 2 * (t / nh) + (par >> 1);
+                    tc_rowmap.push_back((int)(pl->lev_off[l] + (long long)by * (1 << l) + bx));
+                    tc_rowinfo.push_back(make_int4(l, par, t, 0));
+                }
+            }
+        }
+        tc_base[4] = (int)tc_rowmap.size();
+        pl->tc_rows = tc_base[4];
+        pl->tc_maxm = 0;
+        for (int par = 0; par < 4; par++) pl->tc_maxm = std::max(pl->tc_maxm, tc_base[par + 1] - tc_base[par]);
+    }
     int st = MMS_OK;
     if (!st) st = upload(ctx, pl, &pl->Wt, Wt);
     if (!st) st = upload(ctx, pl, &pl->Vt, Vt);
@@ -882,6 +1032,33 @@ int fmm_plan_create(mms_ctx *ctx)
     if (!st) st = upload(ctx, pl, &pl->Tl2l, Tl2l);
     if (!st) st = upload(ctx, pl, &pl->Tm2l, Tm2l);
     if (!st) st = upload(ctx, pl, &pl->Tm2lc, Tm2lc);
+    if (!st && pl->m2l_tc) {
+        st = upload(ctx, pl, &pl->tcB, tcB);
+        if (!st) st = upload(ctx, pl, &pl->tc_rowmap, tc_rowmap);
+        if (!st) st = upload(ctx, pl, &pl->tc_rowinfo, tc_rowinfo);
+        for (int blk = 0; blk < 2 && !st; blk++) {
+            std::vector<__nv_bfloat16> z((size_t)pl->tc_rows * 3 * pl->tcK[blk]);
+            st = upload(ctx, pl, &pl->tcA[blk], z);
+        }
+        if (!st) {
+            std::vector<TcGroup> grp(8);
+            for (int par = 0; par < 4; par++)
+                for (int blk = 0; blk < 2; blk++) {
+                    TcGroup &g = grp[par * 2 + blk];
+                    g.A = pl->tcA[blk] + (size_t)tc_base[par] * 3 * pl->tcK[blk];
+                    g.B = pl->tcB + tcBoff[par * 2 + blk];
+                    g.C = nullptr;  // set at launch: Lpart + block offset
+                    g.rowmap = pl->tc_rowmap + tc_base[par];
+                    g.lda = g.ldb = 3 * pl->tcK[blk];
+                    g.ldc = NR;
+                    g.M = tc_base[par + 1] - tc_base[par];
+                    g.N = blk ? NB1 : NB0;
+                    g.K = 3 * pl->tcK[blk];
+                    g.pad[0] = g.pad[1] = 0;
+                }
+            pl->tc_group_host = grp;  // uploaded once Lpart exists (C pointers)
+        }
+    }
     if (!st) st = upload(ctx, pl, &pl->m2l_items, items);
     long long *lev_dev = nullptr;
     if (!st) st = upload(ctx, pl, &lev_dev, pl->lev_off);
@@ -912,6 +1089,19 @@ int fmm_plan_create(mms_ctx *ctx)
         pl->bytes += (2 + NSPLIT) * ncoef * sizeof(float) + (size_t)Z * 4 * s * s * sizeof(float) +
                      (size_t)ctx->N * sizeof(float);
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Lpart, 0, NSPLIT * ncoef * sizeof(float), ctx->stream));
+        if (pl->m2l_tc) {
+            for (int i = 0; i < 8; i++) pl->tc_group_host[i].C = pl->Lpart + ((i & 1) ? f.NE : 0);
+            if (cudaMalloc((void **)&pl->tc_groups, 8 * sizeof(TcGroup)) != cudaSuccess) {
+                fmm_plan_destroy(ctx);
+                mms_set_error("FMM plan: device allocation failed");
+                return MMS_ERR_NOMEM;
+            }
+            pl->bytes += 8 * sizeof(TcGroup);
+            MMS_CUDA_TRY(cudaMemcpyAsync(pl->tc_groups, pl->tc_group_host.data(), 8 * sizeof(TcGroup),
+                                         cudaMemcpyHostToDevice, ctx->stream));
+            MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2l_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)(sizeof(umma::Smem<64>) + 1024)));
+        }
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Mall, 0, ncoef * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Lall, 0, ncoef * sizeof(float), ctx->stream));
     }
@@ -991,7 +1181,8 @@ void fmm_plan_destroy(mms_ctx *ctx)
     if (!pl) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Tm2lc, pl->Gn, pl->Mall, pl->Lall, pl->Lpart,
-                 pl->m2l_items, pl->lev_dev, pl->near};
+                 pl->m2l_items, pl->lev_dev, pl->near, pl->tcA[0], pl->tcA[1], pl->tcB, pl->tc_rowmap,
+                 pl->tc_rowinfo, pl->tc_groups};
     for (void *p : b)
         if (p) cudaFree(p);
     if (pl->side) cudaStreamSynchronize(pl->side);
@@ -1011,7 +1202,7 @@ static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
     FmmPlan *pl = ctx->fmm;
     const FmmDev &f = pl->d;
     const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
-    const int nsplit = pl->m2l_resident ? 1 : NSPLIT;
+    const int nsplit = (pl->m2l_resident || pl->m2l_tc) ? 1 : NSPLIT;
     const float *Lpar = f.L > 2 ? pl->Lall + pl->lev_off[f.L - 1] * f.NR : nullptr;
     MMS_TRY(l2p_launch(f, nbx, nby, pl->near, pl->Lpart + pl->lev_off[f.L] * f.NR, Lpar, pl->Tl2l, pl->Vt, phi,
                        pl->nbox_total * f.NR, nsplit, ctx->stream));
@@ -1033,7 +1224,7 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     const int thr = ((f.NR + 31) / 32) * 32;
     const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
     const int KT = ((f.NR + 31) / 32) * 32;
-    const int nsplit = pl->m2l_resident ? 1 : NSPLIT;
+    const int nsplit = (pl->m2l_resident || pl->m2l_tc) ? 1 : NSPLIT;
     if (stage < 4 && !far) return MMS_OK;
     switch (stage) {
     case 0: {
@@ -1053,6 +1244,16 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         }
         break;
     case 2: {
+        if (pl->m2l_tc) {
+            k_m2l_gather<<<dim3(pl->tc_rows, 2), 256, 0, ctx->stream>>>(pl->Mall, pl->tcA[0], pl->tcA[1],
+                                                                      pl->tc_rowinfo, pl->lev_dev, f, pl->tcK[0],
+                                                                      pl->tcK[1], pl->tcNBp[0], pl->tcNBp[1]);
+            MMS_LAUNCH_CHECK(ctx);
+            k_m2l_gemm<<<dim3(div_up(pl->tc_maxm, umma::BM), 1, 8), 128, sizeof(umma::Smem<64>) + 1024,
+                         ctx->stream>>>(pl->tc_groups);
+            MMS_LAUNCH_CHECK(ctx);
+            break;
+        }
         if (pl->m2l_resident) {
             MMS_TRY(m2l_res_launch(f, pl->n_m2l_items, pl->Mall, pl->Lpart, pl->Tm2lc, pl->m2l_items, pl->lev_dev,
                                    ctx->stream));

@@ -127,10 +127,11 @@ struct Smem {
 // One 128 x BN tile of C.  A is M x K (lda), B is N x K (ldb), both BF16 with
 // K contiguous; rows beyond M / N and columns beyond K read as zero.
 // beta != 0: C += A B^T, else C = A B^T.  err: set to 1 on a barrier timeout.
+// rowmap (may be NULL): row r of the tile result goes to C row rowmap[r].
 template <int BN>
 __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __nv_bfloat16 *__restrict__ B, int ldb,
                           float *__restrict__ C, int ldc, int M, int N, int K, int m0, int n0, int beta,
-                          int *__restrict__ err, Smem<BN> &s)
+                          int *__restrict__ err, Smem<BN> &s, const int *__restrict__ rowmap = nullptr)
 {
     static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN must be a power of two in [32, 256]");
     const int tid = threadIdx.x;  // 128 threads
@@ -222,7 +223,8 @@ __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
             if (row < M) {
-                float *crow = C + (long long)row * ldc + n0 + c0;
+                const long long crow_i = rowmap ? (long long)rowmap[row] : (long long)row;
+                float *crow = C + crow_i * ldc + n0 + c0;
 #pragma unroll
                 for (int i = 0; i < 16; i++)
                     if (n0 + c0 + i < N) crow[i] = beta ? crow[i] + v[i] : v[i];
@@ -230,8 +232,10 @@ __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __
         }
     } else if (!beta) {
         const int row = m0 + warp * 32 + lane;
-        if (row < M)
-            for (int c = 0; c < BN && n0 + c < N; c++) C[(long long)row * ldc + n0 + c] = 0.f;
+        if (row < M) {
+            const long long crow_i = rowmap ? (long long)rowmap[row] : (long long)row;
+            for (int c = 0; c < BN && n0 + c < N; c++) C[crow_i * ldc + n0 + c] = 0.f;
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();

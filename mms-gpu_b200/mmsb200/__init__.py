@@ -58,7 +58,7 @@ class Params(ctypes.Structure):
 
 class Solver(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("fmm_order", ctypes.c_int), ("fmm_leaf", ctypes.c_int),
-                ("reserved", ctypes.c_int * 5)]
+                ("m2l_mode", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
 
 
 class Controller(ctypes.Structure):
@@ -198,9 +198,12 @@ def make_params(Ms=8.6e5, Aexch=1.3e-11, alpha=0.5, gamma=2.21e5, mu0=4e-7 * np.
     return p, keep
 
 
-def make_solver(kind=SOLVER_DIRECT, order=4, leaf=0):
+M2L_AUTO, M2L_SIMT, M2L_TENSOR = 0, 1, 2
+
+
+def make_solver(kind=SOLVER_DIRECT, order=4, leaf=0, m2l_mode=M2L_AUTO):
     s = Solver()
-    s.kind, s.fmm_order, s.fmm_leaf = kind, order, leaf
+    s.kind, s.fmm_order, s.fmm_leaf, s.m2l_mode = kind, order, leaf, m2l_mode
     return s
 
 

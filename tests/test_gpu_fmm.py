@@ -114,3 +114,23 @@ def test_fmm_bad_order_rejected(cuda, lib):
         fmm_ctx(mmsb200, 16, 16, 3, (5e-9, 5e-9, 5e-9), 0, 4)
     with pytest.raises(mmsb200.MmsError):
         fmm_ctx(mmsb200, 16, 16, 3, (5e-9, 5e-9, 5e-9), 4, 40)
+
+
+@pytest.mark.parametrize("P,s", [(3, 2), (4, 4), (6, 8), (8, 8)])
+def test_tensor_core_m2l(cuda, lib, oracle_mod, P, s):
+    """the tcgen05 split-BF16 M2L (hi*hi + hi*lo + lo*hi) agrees with the FP32
+    SIMT M2L to 3e-5 relative and keeps the FMM within its error bound"""
+    import mmsb200
+    X = Y = 64
+    Z = 3
+    d = (5e-9, 5e-9, 5e-9)
+    g, rho = film_rho(oracle_mod, X, Y, Z, d, 21, masked=0.3)
+    exact = oracle_mod.potential_direct(g, rho)
+    out = {}
+    for mode in (mmsb200.M2L_SIMT, mmsb200.M2L_TENSOR):
+        with mmsb200.Context(mmsb200.Grid(X, Y, Z, *d), mmsb200.make_params(),
+                             mmsb200.make_solver(mmsb200.SOLVER_FMM, P, s, mode)) as ctx:
+            out[mode] = ctx.potential_host(rho)
+    assert rel_l2(out[mmsb200.M2L_TENSOR], out[mmsb200.M2L_SIMT]) < 3e-5
+    # the truncation error is the SIMT path's; the split-BF16 products add < 3e-5
+    assert rel_l2(out[mmsb200.M2L_TENSOR], exact) < rel_l2(out[mmsb200.M2L_SIMT], exact) + 3e-5
