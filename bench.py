@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--solver", choices=["fmm", "direct"], default=os.environ.get("MMS_BENCH_SOLVER", "fmm"))
-    ap.add_argument("--order", type=int, default=4, help="FMM expansion order P")
+    ap.add_argument("--order", type=int, default=0, help="FMM expansion order P (0 = autotuned)")
     ap.add_argument("--leaf", type=int, default=0, help="FMM leaf side in cells (0 = autotuned)")
     ap.add_argument("--m2l", type=int, default=int(os.environ.get("MMS_BENCH_M2L", "0")),
                     help="FMM M2L: 0 auto, 1 FP32 SIMT, 2 tensor cores (split BF16)")
@@ -234,6 +234,18 @@ def run_ours(args):
     params = mmsb200.make_params(external=True, hext_t=hext_t, hext_b=hext_b)
     kind = mmsb200.SOLVER_FMM if args.solver == "fmm" else mmsb200.SOLVER_DIRECT
     solver = mmsb200.make_solver(kind, args.order, args.leaf, args.m2l)
+    tuned = None
+    if kind == mmsb200.SOLVER_FMM and args.order == 0:
+        # autotuned: fastest (P, leaf, M2L kernel) within half the metric's 1e-3 target
+        Mf = torch.from_numpy(M.astype(np.float32)).cuda()
+        rho0 = torch.empty((Z, Y, X), dtype=torch.float32, device="cuda")
+        with mmsb200.Context(grid, params, mmsb200.make_solver(mmsb200.SOLVER_DIRECT)) as tctx:
+            tctx.divergence_dev(Mf, rho0)
+            tctx.sync()
+        solver, tms, terr = mmsb200.autotune_fmm(grid, params, rho0, 5e-4)
+        tuned = {"P": solver.fmm_order, "leaf": solver.fmm_leaf, "m2l": solver.m2l_mode, "ms": tms, "err": terr}
+        args.order, args.leaf, args.m2l = solver.fmm_order, solver.fmm_leaf, solver.m2l_mode
+        del Mf, rho0
     # a dedicated stream: the library's kernels and every timing event live on it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -363,7 +375,7 @@ def run_ours(args):
            f"({L2_FLUSH_BYTES >> 20} MB write, outside the timed events)", "graph": "one CUDA graph per RK4 step",
            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
     if args.solver == "fmm":
-        cfg.update({"P": args.order, "leaf": args.leaf or "auto",
+        cfg.update({"P": args.order, "leaf": args.leaf or "auto", "autotune": tuned,
                     "m2l": {0: "auto", 1: "fp32 simt", 2: "tensor cores (split bf16)"}[args.m2l]})
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,

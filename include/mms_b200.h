@@ -230,6 +230,17 @@ int mms_ens_sync(mms_ens *ens);
 int mms_potential_direct_noalloc(const float *rho, float *phi, int xdim, int ydim, int zdim,
                                  double dx, double dy, double dz, void *stream);
 
+/* autotuner ------------------------------------------------------------------ */
+/* Chooses the FMM order P (3..8), leaf side (4, 8) and M2L kernel for a grid by
+ * measurement: each candidate evaluates the potential of rho_dev (a device
+ * charge density of the grid), its rel-L2 error against the exact direct sum
+ * (computed on the same device) must be <= max_rel_err, and the fastest such
+ * candidate (mean of `reps` evaluations, CUDA events) is returned in *best.
+ * Cached per process by (grid, cell size, target).  No reference
+ * counterpart (the reference hard-codes P, main.cpp:31). */
+int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, const float *rho_dev, double max_rel_err,
+                     int reps, mms_solver *best, double *best_ms, double *best_err);
+
 /* diagnostics ---------------------------------------------------------------- */
 /* The library's tcgen05 tensor-core GEMM on BF16 operands: C = A B^T (beta 0)
  * or C += A B^T (beta 1); A M x K and B N x K row-major (K contiguous), C

@@ -1,0 +1,175 @@
+// Autotuner: picks the FMM expansion order, leaf side and M2L kernel for a
+// grid by measurement.  Every candidate evaluates the potential of a sample
+// charge density; its error is judged against the exact direct sum computed
+// on the same device (FP32 table + compensated sums, within 2e-6 of FP64),
+// and the fastest candidate within the error target wins.  Results are cached
+// in-process per shape class (grid dims, cell size, target).
+#include <math.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "mms_internal.cuh"
+
+namespace {
+
+__global__ void k_diff_norm(const float *__restrict__ a, const float *__restrict__ b, long long n,
+                            double *__restrict__ out)
+{
+    __shared__ double sd[2][8];
+    double d2 = 0.0, b2 = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double x = a[i], y = b[i];
+        d2 += (x - y) * (x - y);
+        b2 += y * y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+        b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sd[0][threadIdx.x >> 5] = d2;
+        sd[1][threadIdx.x >> 5] = b2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0, a1 = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            a0 += sd[0][w];
+            a1 += sd[1][w];
+        }
+        out[2 * blockIdx.x] = a0;
+        out[2 * blockIdx.x + 1] = a1;
+    }
+}
+
+struct Key {
+    int X, Y, Z;
+    long long dxq, dyq, dzq, tolq;
+    bool operator<(const Key &o) const
+    {
+        return std::tie(X, Y, Z, dxq, dyq, dzq, tolq) < std::tie(o.X, o.Y, o.Z, o.dxq, o.dyq, o.dzq, o.tolq);
+    }
+};
+
+struct Result {
+    mms_solver s;
+    double ms, err;
+};
+
+std::mutex g_mu;
+std::map<Key, Result> g_cache;
+
+}  // namespace
+
+extern "C" int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, const float *rho_dev,
+                                double max_rel_err, int reps, mms_solver *best, double *best_ms, double *best_err)
+{
+    if (!grid || !params || !rho_dev || !best || !(max_rel_err > 0)) {
+        mms_set_error("mms_autotune_fmm: bad argument");
+        return MMS_ERR_ARG;
+    }
+    if (reps < 1) reps = 5;
+    const Key key{grid->xdim, grid->ydim, grid->zdim, llround(grid->dx * 1e15), llround(grid->dy * 1e15),
+                  llround(grid->dz * 1e15), llround(log10(max_rel_err) * 100)};
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) {
+            *best = it->second.s;
+            if (best_ms) *best_ms = it->second.ms;
+            if (best_err) *best_err = it->second.err;
+            return MMS_OK;
+        }
+    }
+    mms_solver dsolv;
+    memset(&dsolv, 0, sizeof dsolv);
+    dsolv.kind = MMS_SOLVER_DIRECT;
+    mms_ctx *ctx = nullptr;
+    MMS_TRY(mms_ctx_create(grid, params, &dsolv, nullptr, &ctx));
+    const long long N = ctx->N;
+    float *exact = nullptr, *phi = nullptr;
+    double *part = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int st = MMS_OK;
+    Result bestr{};
+    bestr.ms = 1e300;
+    bool found = false;
+    do {
+        if ((st = ctx_alloc(ctx, &exact, (size_t)N)) || (st = ctx_alloc(ctx, &phi, (size_t)N)) ||
+            (st = ctx_alloc(ctx, &part, 2 * 256)))
+            break;
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+            st = MMS_ERR_CUDA;
+            mms_set_error("event creation failed");
+            break;
+        }
+        if ((st = launch_potential_direct(ctx, rho_dev, exact))) break;
+        const int orders[] = {3, 4, 5, 6, 7, 8};
+        const int leaves[] = {4, 8};
+        const int modes[] = {1, 2};
+        std::vector<double> h(2 * 256);
+        for (int P : orders)
+            for (int s : leaves)
+                for (int m : modes) {
+                    mms_solver c;
+                    memset(&c, 0, sizeof c);
+                    c.kind = MMS_SOLVER_FMM;
+                    c.fmm_order = P;
+                    c.fmm_leaf = s;
+                    c.m2l_mode = m;
+                    if (mms_ctx_set_solver(ctx, &c) != MMS_OK) continue;  // unsupported combination
+                    if (launch_potential(ctx, rho_dev, phi) != MMS_OK) continue;
+                    k_diff_norm<<<256, 256, 0, ctx->stream>>>(phi, exact, N, part);
+                    if (cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                        ctx->stream) != cudaSuccess ||
+                        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+                        st = MMS_ERR_CUDA;
+                        mms_set_error("autotune: %s", cudaGetErrorString(cudaGetLastError()));
+                        break;
+                    }
+                    double d2 = 0, b2 = 0;
+                    for (int i = 0; i < 256; i++) {
+                        d2 += h[2 * i];
+                        b2 += h[2 * i + 1];
+                    }
+                    const double err = b2 > 0 ? sqrt(d2 / b2) : 0.0;
+                    if (!(err <= max_rel_err)) continue;
+                    cudaEventRecord(e0, ctx->stream);
+                    for (int r = 0; r < reps; r++) launch_potential(ctx, rho_dev, phi);
+                    cudaEventRecord(e1, ctx->stream);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    const double t = (double)ms / reps;
+                    if (t < bestr.ms) {
+                        bestr.s = c;
+                        bestr.ms = t;
+                        bestr.err = err;
+                        found = true;
+                    }
+                }
+    } while (0);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (exact) cudaFree(exact);
+    if (phi) cudaFree(phi);
+    if (part) cudaFree(part);
+    mms_ctx_destroy(ctx);
+    if (st != MMS_OK) return st;
+    if (!found) {
+        mms_set_error("autotune: no FMM configuration reaches rel-L2 %g on this grid", max_rel_err);
+        return MMS_ERR_ARG;
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_cache[key] = bestr;
+    }
+    *best = bestr.s;
+    if (best_ms) *best_ms = bestr.ms;
+    if (best_err) *best_err = bestr.err;
+    return MMS_OK;
+}

@@ -105,6 +105,8 @@ SIGNATURES = {
     "mms_march": (_I, [_VP, ctypes.POINTER(Controller), _D, _D, ctypes.POINTER(Record), _I, ctypes.POINTER(_I),
                        MARCH_CB, _VP]),
     "mms_diag_fma_tflops": (_I, [_I, ctypes.POINTER(_D)]),
+    "mms_autotune_fmm": (_I, [ctypes.POINTER(Grid), ctypes.POINTER(Params), _VP, _D, _I, ctypes.POINTER(Solver),
+                              ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "mms_diag_gemm_bf16": (_I, [_VP, _I, _VP, _I, _VP, _I, _I, _I, _I, _I, _I, _VP]),
     "mms_potential_direct_noalloc": (_I, [_VP, _VP, _I, _I, _I, _D, _D, _D, _VP]),
     "mms_ens_create": (_I, [_VP, _I, _D, _D, _D, ctypes.POINTER(Params), _VP, ctypes.POINTER(_VP)]),
@@ -177,6 +179,18 @@ def fmm_stage_times(ctx, rho, phi, reps=10):
     out = (ctypes.c_double * 5)()
     _check(load().mms_fmm_stage_times(ctx.h, _ptr(rho), _ptr(phi), reps, out))
     return dict(zip(("p2m", "m2m", "m2l", "l2l", "l2p_p2p"), list(out)))
+
+
+def autotune_fmm(grid, params, rho_dev, max_rel_err=5e-4, reps=5):
+    """fastest FMM solver for `grid` within `max_rel_err` of the exact sum on
+    the sample charge density `rho_dev` (device tensor); returns
+    (Solver, ms per potential, rel-L2 error)"""
+    p = params[0] if isinstance(params, tuple) else params
+    best = Solver()
+    ms, err = ctypes.c_double(), ctypes.c_double()
+    _check(load().mms_autotune_fmm(ctypes.byref(grid), ctypes.byref(p), _ptr(rho_dev), max_rel_err, reps,
+                                   ctypes.byref(best), ctypes.byref(ms), ctypes.byref(err)))
+    return best, ms.value, err.value
 
 
 def make_params(Ms=8.6e5, Aexch=1.3e-11, alpha=0.5, gamma=2.21e5, mu0=4e-7 * np.pi, demag=True, exchange=True,

@@ -134,3 +134,27 @@ def test_tensor_core_m2l(cuda, lib, oracle_mod, P, s):
     assert rel_l2(out[mmsb200.M2L_TENSOR], out[mmsb200.M2L_SIMT]) < 3e-5
     # the truncation error is the SIMT path's; the split-BF16 products add < 3e-5
     assert rel_l2(out[mmsb200.M2L_TENSOR], exact) < rel_l2(out[mmsb200.M2L_SIMT], exact) + 3e-5
+
+
+def test_autotune_meets_target(cuda, lib, oracle_mod):
+    """the autotuner's pick reaches its error target against the FP64 sum, and
+    a second call is answered from the cache with the same solver"""
+    import torch
+    import mmsb200
+    from mmsb200 import geometry
+    mask = geometry.random_blocks_mask(96, 80, 3, 0.2, 4, 77)
+    M = geometry.random_inplane(mask, 78)
+    g = oracle_mod.Grid(96, 80, 3, 5e-9, 5e-9, 5e-9)
+    rho = oracle_mod.divergence(g, M).astype(np.float32)
+    exact = oracle_mod.potential_direct(g, rho)
+    grid = mmsb200.Grid(96, 80, 3, 5e-9, 5e-9, 5e-9)
+    params = mmsb200.make_params()
+    rho_dev = torch.from_numpy(rho).cuda()
+    target = 2e-4
+    s1, ms1, err1 = mmsb200.autotune_fmm(grid, params, rho_dev, target)
+    s2, ms2, err2 = mmsb200.autotune_fmm(grid, params, rho_dev, target)
+    assert s1.kind == mmsb200.SOLVER_FMM and err1 <= target and ms1 > 0
+    assert (s1.fmm_order, s1.fmm_leaf, s1.m2l_mode) == (s2.fmm_order, s2.fmm_leaf, s2.m2l_mode) and ms1 == ms2
+    with mmsb200.Context(grid, params, s1) as ctx:
+        phi = ctx.potential_host(rho)
+    assert rel_l2(phi, exact) <= 1.05 * target
