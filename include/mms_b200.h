@@ -53,7 +53,11 @@ typedef enum {
 
 typedef enum {
     MMS_SOLVER_DIRECT = 0,   /* exact O(N^2) sum, FP32 tiles, compensated      */
-    MMS_SOLVER_FMM = 1       /* spherical-harmonic FMM, exact near field       */
+    MMS_SOLVER_FMM = 1,      /* spherical-harmonic FMM, exact near field       */
+    MMS_SOLVER_SURROGATE = 2 /* exact near field (FMM P2P, leaf 4) + far field
+                                from the learned operator (mms_sno_*); the FMM
+                                of the same order checks it and takes over
+                                (mms_ctx_set_surrogate)                       */
 } mms_solver_kind;
 
 typedef struct {
@@ -240,6 +244,53 @@ int mms_potential_direct_noalloc(const float *rho, float *phi, int xdim, int ydi
  * counterpart (the reference hard-codes P, main.cpp:31). */
 int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, const float *rho_dev, double max_rel_err,
                      int reps, mms_solver *best, double *best_ms, double *best_err);
+
+/* surrogate far field ---------------------------------------------------------
+ * A 3-D convolutional neural operator (U-Net over the 4 x 4-cell patch grid,
+ * 4 levels, 32 channels, BF16 weights, FP32 accumulation, no biases or
+ * activations: the map is linear) from the dimensionless cell charge
+ * u = rho dx / Ms to the dimensionless far-field potential
+ * phi_far / (Ms dx) for cubic cells, where phi_far = phi - (exact near field
+ * over the 3 x 3 leaf-box neighbourhood, leaf side 4, all layers).  Forward,
+ * backward and the optimiser are the library's own tcgen05 kernels.  No
+ * reference counterpart (the reference has no learned component). */
+typedef struct mms_sno mms_sno;
+long long mms_sno_num_params(void);
+/* a network for [batch][zdim][ydim][xdim] cell arrays on the current device */
+int mms_sno_create(int xdim, int ydim, int zdim, int batch, mms_sno **out);
+void mms_sno_destroy(mms_sno *net);
+/* FP32 master weights, host arrays of mms_sno_num_params() values; per layer
+ * [cout][tap][cin] in layer order.  get with bf16_rounded != 0 returns the
+ * BF16 values the kernels use. */
+int mms_sno_set_weights(mms_sno *net, const float *w, long long count);
+int mms_sno_get_weights(mms_sno *net, float *w, long long count, int bf16_rounded);
+/* out = network(u) for nbatch <= batch samples (device arrays, legacy stream) */
+int mms_sno_forward_dev(mms_sno *net, const float *u, float *out, int nbatch);
+/* loss = mean_b |net(u_b) - far_b|^2 / |far_b|^2 and its gradient w.r.t. the
+ * FP32 weights (host array, may be NULL); device inputs */
+int mms_sno_gradient(mms_sno *net, const float *u, const float *far, int nbatch, float *grad, double *loss);
+/* one Adam step on that loss; *loss is the loss before the step */
+int mms_sno_train_step(mms_sno *net, const float *u, const float *far, int nbatch, float lr, float beta1,
+                       float beta2, float eps, double *loss);
+long long mms_sno_device_bytes(const mms_sno *net);
+
+/* Binds trained weights to a context whose solver is MMS_SOLVER_SURROGATE and
+ * arms its check: every `check_every` steps (0: never) of mms_run_fixed, and
+ * every `check_every` accepted steps plus every rejected step of mms_march,
+ * the potential of the current state is computed by both the surrogate and
+ * the FMM (the solver's order, leaf 4); when their rel-L2 difference exceeds
+ * `tol` the FMM replaces the surrogate for the rest of the run.  Cubic cells
+ * only. */
+int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol);
+/* runs that check now on the current state; *err = rel-L2(surrogate, FMM) */
+int mms_surrogate_check(mms_ctx *ctx, double *err);
+/* active: 1 while the surrogate is in use, 0 after the FMM took over */
+int mms_surrogate_stats(const mms_ctx *ctx, int *active, long long *checks, long long *fallbacks,
+                        double *last_err, double *max_err);
+/* far-field split of the FMM potential: phi = FMM(rho) and near = its exact
+ * near-field part (leaf-box neighbourhood P2P); context solver must be
+ * MMS_SOLVER_FMM or MMS_SOLVER_SURROGATE (device arrays of N floats) */
+int mms_potential_split_dev(mms_ctx *ctx, const float *rho, float *phi, float *near);
 
 /* diagnostics ---------------------------------------------------------------- */
 /* The library's tcgen05 tensor-core GEMM on BF16 operands: C = A B^T (beta 0)

@@ -175,6 +175,13 @@ int ensure_phi(mms_ctx *ctx)
     return MMS_OK;
 }
 
+// the solver a captured graph holds: the surrogate solver runs the FMM once it took over
+int effective_kind(const mms_ctx *ctx)
+{
+    if (ctx->s.kind == MMS_SOLVER_SURROGATE && !ctx->sur_active) return MMS_SOLVER_FMM;
+    return ctx->s.kind;
+}
+
 int run_steps(mms_ctx *ctx, int nsteps, int use_graph)
 {
     MMS_TRY(ensure_phi(ctx));
@@ -182,7 +189,8 @@ int run_steps(mms_ctx *ctx, int nsteps, int use_graph)
         for (int s = 0; s < nsteps; s++) MMS_TRY(rk4_step_kernels(ctx));
         return MMS_OK;
     }
-    if (ctx->graph_exec && ctx->graph_solver_kind != ctx->s.kind) drop_graph(ctx);
+    const int kind = effective_kind(ctx);
+    if (ctx->graph_exec && ctx->graph_solver_kind != kind) drop_graph(ctx);
     if (!ctx->graph_exec) {
         const int64_t before = ctx->launches;
         MMS_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -201,13 +209,44 @@ int run_steps(mms_ctx *ctx, int nsteps, int use_graph)
         MMS_CUDA_TRY(cudaGraphInstantiate(&ctx->graph_exec, graph, 0));
         ctx->graph_kernels = (int)(ctx->launches - before);
         ctx->launches = before;  // captured, not yet launched
-        ctx->graph_solver_kind = ctx->s.kind;
+        ctx->graph_solver_kind = kind;
     }
     for (int s = 0; s < nsteps; s++) {
         MMS_CUDA_TRY(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
         ctx->launches += ctx->graph_kernels;
     }
     return MMS_OK;
+}
+
+// surrogate check on the current state: both potentials, rel-L2, fallback
+int surrogate_check_now(mms_ctx *ctx, double *err_out)
+{
+    MMS_TRY(launch_divergence_soa(ctx, ctx->M, ctx->rho));
+    float *ps = ctx->vecA, *pf = ctx->vecB;
+    MMS_TRY(launch_potential_surrogate(ctx, ctx->rho, ps));
+    MMS_TRY(launch_potential_fmm(ctx, ctx->rho, pf));
+    double err = 0;
+    MMS_TRY(rel_l2_dev(ctx, ps, pf, ctx->N, &err));
+    MMS_TRY(sno_error_flag(ctx->sno, ctx->stream));
+    ctx->sur_checks++;
+    ctx->sur_last_err = err;
+    ctx->sur_max_err = std::max(ctx->sur_max_err, err);
+    ctx->sur_since = 0;
+    if (!(err <= ctx->sur_tol) && ctx->sur_active) {
+        ctx->sur_active = false;
+        ctx->sur_fallbacks++;
+        // from here on phi is the FMM's potential of M
+        MMS_CUDA_TRY(cudaMemcpyAsync(ctx->phi, pf, (size_t)ctx->N * sizeof(float), cudaMemcpyDeviceToDevice,
+                                     ctx->stream));
+        drop_graph(ctx);
+    }
+    if (err_out) *err_out = err;
+    return MMS_OK;
+}
+
+bool surrogate_armed(const mms_ctx *ctx)
+{
+    return ctx->s.kind == MMS_SOLVER_SURROGATE && ctx->sno && ctx->sur_active && ctx->sur_every > 0;
 }
 
 int read_stats(mms_ctx *ctx, double out[STAT_SLOTS])
@@ -251,6 +290,8 @@ int clear_numeric_flag(mms_ctx *ctx)
 
 int launch_potential(mms_ctx *ctx, const float *rho, float *phi)
 {
+    if (ctx->s.kind == MMS_SOLVER_SURROGATE)
+        return ctx->sur_active ? launch_potential_surrogate(ctx, rho, phi) : launch_potential_fmm(ctx, rho, phi);
     if (ctx->s.kind == MMS_SOLVER_FMM) return launch_potential_fmm(ctx, rho, phi);
     return launch_potential_direct(ctx, rho, phi);
 }
@@ -331,7 +372,7 @@ int mms_ctx_create(const mms_grid *grid, const mms_params *params, const mms_sol
         def.kind = MMS_SOLVER_DIRECT;
         def.fmm_order = 4;
         ctx->s = solver ? *solver : def;
-        if (ctx->s.kind == MMS_SOLVER_FMM) {
+        if (ctx->s.kind == MMS_SOLVER_FMM || ctx->s.kind == MMS_SOLVER_SURROGATE) {
             if ((st = fmm_plan_create(ctx))) break;
         } else if (ctx->s.kind == MMS_SOLVER_DIRECT) {
             if ((st = direct_build_table(ctx))) break;
@@ -364,6 +405,7 @@ int mms_ctx_destroy(mms_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     drop_graph(ctx);
     fmm_plan_destroy(ctx);
+    if (ctx->sno) mms_sno_destroy(ctx->sno);
     void *bufs[] = {ctx->rho, ctx->phi, ctx->phibak, ctx->vecA, ctx->vecB, ctx->gtab, ctx->mat, ctx->M, ctx->A,
                     ctx->B, ctx->K, ctx->Mbak, ctx->Mfull, ctx->tstate, ctx->hext, ctx->stat_part, ctx->stats};
     for (void *b : bufs)
@@ -396,7 +438,7 @@ int mms_ctx_set_solver(mms_ctx *ctx, const mms_solver *solver)
     drop_graph(ctx);
     fmm_plan_destroy(ctx);
     ctx->s = *solver;
-    if (ctx->s.kind == MMS_SOLVER_FMM) {
+    if (ctx->s.kind == MMS_SOLVER_FMM || ctx->s.kind == MMS_SOLVER_SURROGATE) {
         MMS_TRY(fmm_plan_create(ctx));
     } else if (ctx->s.kind == MMS_SOLVER_DIRECT) {
         if (!ctx->gtab) MMS_TRY(direct_build_table(ctx));
@@ -597,7 +639,15 @@ int mms_run_fixed(mms_ctx *ctx, double dt, int nsteps, int use_graph)
     }
     k_set_dt<<<1, 1, 0, ctx->stream>>>(ctx->tstate, dt);
     MMS_LAUNCH_CHECK(ctx);
-    return run_steps(ctx, nsteps, use_graph);
+    int left = nsteps;
+    while (left > 0 && surrogate_armed(ctx)) {
+        const int chunk = (int)std::min<long long>(left, ctx->sur_every - ctx->sur_since);
+        MMS_TRY(run_steps(ctx, chunk, use_graph));
+        left -= chunk;
+        ctx->sur_since += chunk;
+        if (ctx->sur_since >= ctx->sur_every) MMS_TRY(surrogate_check_now(ctx, nullptr));
+    }
+    return (left > 0 || nsteps == 0) ? run_steps(ctx, left, use_graph) : MMS_OK;
 }
 
 int mms_state_stats(mms_ctx *ctx, double *E_eV, double *torque, double Mavg[3], double *Mmag_avg)
@@ -709,6 +759,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
             const double torque = st[1] / Ms / Ms;
             if (E2 - E > 0.1) {  // reject: energy rose by more than 0.1 eV
                 MMS_TRY(restore(t, tk1));
+                if (surrogate_armed(ctx)) MMS_TRY(surrogate_check_now(ctx, nullptr));
                 dt = dt / 2.5;
                 if (report_reject(dt, E2, torque)) break;
                 if (++rejects > max_rejects) {
@@ -719,6 +770,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
                 continue;
             }
             rejects = 0;
+            if (surrogate_armed(ctx) && ++ctx->sur_since >= ctx->sur_every) MMS_TRY(surrogate_check_now(ctx, nullptr));
             t = t + dt;                   // the step just taken
             dt = 1e-14 / torque / 2;      // ode_functions.cpp:298-299
             tindex++;
@@ -761,6 +813,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
             if (dtmin > 0) hnew = std::max(hnew, dtmin);
             if (!(err <= rtol) && !(dtmin > 0 && h <= dtmin)) {
                 MMS_TRY(restore(t, tk1));
+                if (surrogate_armed(ctx)) MMS_TRY(surrogate_check_now(ctx, nullptr));
                 dt = hnew;
                 if (report_reject(dt, 0.0, 0.0)) break;
                 if (++rejects > max_rejects) {
@@ -771,6 +824,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
                 continue;
             }
             rejects = 0;
+            if (surrogate_armed(ctx) && ++ctx->sur_since >= ctx->sur_every) MMS_TRY(surrogate_check_now(ctx, nullptr));
             t += h;
             tindex++;
             dt = hnew;
@@ -787,6 +841,77 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
     }
     if (n_records) *n_records = nrec;
     return status;
+}
+
+
+// ---- surrogate solver ------------------------------------------------------------
+
+int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol)
+{
+    if (!ctx || !w || check_every < 0 || !(tol > 0)) {
+        mms_set_error("mms_ctx_set_surrogate: bad argument");
+        return MMS_ERR_ARG;
+    }
+    if (ctx->s.kind != MMS_SOLVER_SURROGATE) {
+        mms_set_error("mms_ctx_set_surrogate: the context's solver is not MMS_SOLVER_SURROGATE");
+        return MMS_ERR_ARG;
+    }
+    if (fabs(ctx->g.dy / ctx->g.dx - 1.0) > 1e-9 || fabs(ctx->g.dz / ctx->g.dx - 1.0) > 1e-9) {
+        mms_set_error("mms_ctx_set_surrogate: the network is trained for cubic cells");
+        return MMS_ERR_ARG;
+    }
+    MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (!ctx->sno) {
+        MMS_TRY(mms_sno_create(ctx->g.xdim, ctx->g.ydim, ctx->g.zdim, 1, &ctx->sno));
+        ctx->dev_bytes += (size_t)mms_sno_device_bytes(ctx->sno);
+    }
+    MMS_TRY(mms_sno_set_weights(ctx->sno, w, count));
+    ctx->sur_every = check_every;
+    ctx->sur_tol = tol;
+    ctx->sur_active = true;
+    ctx->sur_since = ctx->sur_checks = ctx->sur_fallbacks = 0;
+    ctx->sur_last_err = ctx->sur_max_err = 0;
+    drop_graph(ctx);
+    ctx->phi_valid = false;
+    return MMS_OK;
+}
+
+int mms_surrogate_check(mms_ctx *ctx, double *err)
+{
+    MMS_TRY(require_state(ctx));
+    if (ctx->s.kind != MMS_SOLVER_SURROGATE || !ctx->sno) {
+        mms_set_error("mms_surrogate_check: no surrogate bound to this context");
+        return MMS_ERR_ARG;
+    }
+    return surrogate_check_now(ctx, err);
+}
+
+int mms_surrogate_stats(const mms_ctx *ctx, int *active, long long *checks, long long *fallbacks, double *last_err,
+                        double *max_err)
+{
+    if (!ctx) {
+        mms_set_error("context is NULL");
+        return MMS_ERR_ARG;
+    }
+    if (active) *active = ctx->s.kind == MMS_SOLVER_SURROGATE && ctx->sno && ctx->sur_active;
+    if (checks) *checks = ctx->sur_checks;
+    if (fallbacks) *fallbacks = ctx->sur_fallbacks;
+    if (last_err) *last_err = ctx->sur_last_err;
+    if (max_err) *max_err = ctx->sur_max_err;
+    return MMS_OK;
+}
+
+int mms_potential_split_dev(mms_ctx *ctx, const float *rho, float *phi, float *near)
+{
+    if (!ctx || !rho || !phi || !near) {
+        mms_set_error("NULL argument");
+        return MMS_ERR_ARG;
+    }
+    if (ctx->s.kind != MMS_SOLVER_FMM && ctx->s.kind != MMS_SOLVER_SURROGATE) {
+        mms_set_error("mms_potential_split_dev: needs an FMM plan");
+        return MMS_ERR_ARG;
+    }
+    return launch_potential_split(ctx, rho, phi, near);
 }
 
 }  // extern "C"

@@ -833,7 +833,11 @@ int fmm_plan_create(mms_ctx *ctx)
         return MMS_ERR_ARG;
     }
     int s = ctx->s.fmm_leaf;
-    if (s == 0) s = fmm_default_leaf(P, ctx->g.xdim, ctx->g.ydim);
+    if (s == 0) s = ctx->s.kind == MMS_SOLVER_SURROGATE ? 4 : fmm_default_leaf(P, ctx->g.xdim, ctx->g.ydim);
+    if (ctx->s.kind == MMS_SOLVER_SURROGATE && s != 4) {
+        mms_set_error("the surrogate solver needs leaf side 4 (its patch), got %d", s);
+        return MMS_ERR_ARG;
+    }
     if (s < 1 || s > 16) {
         mms_set_error("FMM leaf side must be 1..16 cells (got %d)", s);
         return MMS_ERR_ARG;
@@ -1333,6 +1337,44 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
     for (int st = 0; st < 4; st++) MMS_TRY(launch_fmm_stage(ctx, st, rho, phi));
     MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
     return l2p_launch_far(ctx, rho, phi);
+}
+
+// surrogate potential: the exact near field on the side stream, the learned
+// far field on the main one; the network's last layer adds the two
+int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
+{
+    FmmPlan *pl = ctx->fmm;
+    if (!pl || !ctx->sno) {
+        mms_set_error("surrogate solver: no weights bound (mms_ctx_set_surrogate)");
+        return MMS_ERR_NOT_READY;
+    }
+    const FmmDev &f = pl->d;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    MMS_CUDA_TRY(cudaEventRecord(pl->ev_fork, ctx->stream));
+    MMS_CUDA_TRY(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
+    MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, pl->side));
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
+    // u = rho dx / Ms in, phi_far = (Ms dx) y out (cubic cells)
+    const double Ms = ctx->p.Ms > 0 ? ctx->p.Ms : 1.0;
+    return sno_launch_far(ctx->sno, ctx->stream, rho, (float)(ctx->g.dx / Ms), phi, pl->near,
+                          (float)(Ms * ctx->g.dx), pl->ev_join, &ctx->launches);
+}
+
+// FMM potential and its exact near-field part (for the surrogate's targets)
+int launch_potential_split(mms_ctx *ctx, const float *rho, float *phi, float *near)
+{
+    FmmPlan *pl = ctx->fmm;
+    if (!pl || leaf_threads(pl->d) == 0) {
+        mms_set_error("potential split: needs an FMM plan with a power-of-two leaf side");
+        return MMS_ERR_ARG;
+    }
+    MMS_TRY(launch_potential_fmm(ctx, rho, phi));
+    const FmmDev &f = pl->d;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, near, ctx->stream));
+    MMS_LAUNCH_CHECK(ctx);
+    return MMS_OK;
 }
 
 int fmm_default_leaf(int P, int X, int Y)

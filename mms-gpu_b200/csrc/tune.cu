@@ -46,6 +46,34 @@ __global__ void k_diff_norm(const float *__restrict__ a, const float *__restrict
     }
 }
 
+}  // namespace
+
+int rel_l2_dev(mms_ctx *ctx, const float *a, const float *b, long long n, double *out)
+{
+    static thread_local double *part = nullptr;
+    static thread_local int part_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!part || part_dev != dev) {
+        MMS_CUDA_TRY(cudaMalloc(&part, 2 * 256 * sizeof(double)));
+        part_dev = dev;
+    }
+    double h[2 * 256];
+    k_diff_norm<<<256, 256, 0, ctx->stream>>>(a, b, n, part);
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_CUDA_TRY(cudaMemcpyAsync(h, part, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    double d2 = 0, b2 = 0;
+    for (int i = 0; i < 256; i++) {
+        d2 += h[2 * i];
+        b2 += h[2 * i + 1];
+    }
+    *out = b2 > 0 ? sqrt(d2 / b2) : 0.0;
+    return MMS_OK;
+}
+
+namespace {
+
 struct Key {
     int X, Y, Z;
     long long dxq, dyq, dzq, tolq;

@@ -25,7 +25,7 @@ LIB_PATH = os.path.join(LIB_DIR, "libmms_b200.so")
 REFAPI_PATH = os.path.join(LIB_DIR, "libmms_refapi.so")
 
 MMS_OK, MMS_ERR_ARG, MMS_ERR_CUDA, MMS_ERR_NOMEM, MMS_ERR_NUMERIC, MMS_ERR_NOT_READY, MMS_ERR_REJECTED = range(7)
-SOLVER_DIRECT, SOLVER_FMM = 0, 1
+SOLVER_DIRECT, SOLVER_FMM, SOLVER_SURROGATE = 0, 1, 2
 
 
 class MmsError(RuntimeError):
@@ -118,6 +118,21 @@ SIGNATURES = {
     "mms_ens_run_fixed": (_I, [_VP, _D, _I, _I]),
     "mms_ens_sync": (_I, [_VP]),
     "mms_fmm_stage_times": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_D)]),
+    "mms_sno_num_params": (ctypes.c_longlong, []),
+    "mms_sno_create": (_I, [_I, _I, _I, _I, ctypes.POINTER(_VP)]),
+    "mms_sno_destroy": (None, [_VP]),
+    "mms_sno_set_weights": (_I, [_VP, _VP, ctypes.c_longlong]),
+    "mms_sno_get_weights": (_I, [_VP, _VP, ctypes.c_longlong, _I]),
+    "mms_sno_forward_dev": (_I, [_VP, _VP, _VP, _I]),
+    "mms_sno_gradient": (_I, [_VP, _VP, _VP, _I, _VP, ctypes.POINTER(_D)]),
+    "mms_sno_train_step": (_I, [_VP, _VP, _VP, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                ctypes.POINTER(_D)]),
+    "mms_sno_device_bytes": (ctypes.c_longlong, [_VP]),
+    "mms_ctx_set_surrogate": (_I, [_VP, _VP, ctypes.c_longlong, _I, _D]),
+    "mms_surrogate_check": (_I, [_VP, ctypes.POINTER(_D)]),
+    "mms_surrogate_stats": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong),
+                                 ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "mms_potential_split_dev": (_I, [_VP, _VP, _VP, _VP]),
     "mms_fmm_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D),
                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
 }
@@ -290,6 +305,26 @@ class Context:
     def potential_dev(self, rho, phi):
         _check(load().mms_potential_dev(self.h, _ptr(rho), _ptr(phi)))
 
+    def potential_split_dev(self, rho, phi, near):
+        """FMM potential and its exact near-field part (device arrays)"""
+        _check(load().mms_potential_split_dev(self.h, _ptr(rho), _ptr(phi), _ptr(near)))
+
+    def set_surrogate(self, weights, check_every=50, tol=1e-3):
+        w = np.ascontiguousarray(weights, np.float32)
+        _check(load().mms_ctx_set_surrogate(self.h, _ptr(w), w.size, check_every, tol))
+
+    def surrogate_check(self):
+        e = ctypes.c_double()
+        _check(load().mms_surrogate_check(self.h, ctypes.byref(e)))
+        return e.value
+
+    def surrogate_stats(self):
+        a, c, f = ctypes.c_int(), ctypes.c_longlong(), ctypes.c_longlong()
+        le, me = ctypes.c_double(), ctypes.c_double()
+        _check(load().mms_surrogate_stats(self.h, ctypes.byref(a), ctypes.byref(c), ctypes.byref(f),
+                                          ctypes.byref(le), ctypes.byref(me)))
+        return dict(active=bool(a.value), checks=c.value, fallbacks=f.value, last_err=le.value, max_err=me.value)
+
     def gradient_dev(self, phi, c, H):
         _check(load().mms_gradient_dev(self.h, _ptr(phi), c, _ptr(H)))
 
@@ -359,3 +394,65 @@ class Context:
         if st not in (MMS_OK, MMS_ERR_REJECTED):
             _check(st)
         return rows, st
+
+
+class SNO:
+    """The surrogate far-field network (mms_sno) for [batch][Z][Y][X] cell
+    arrays on the current CUDA device: dimensionless charge u = rho dx / Ms in,
+    dimensionless far-field potential phi_far / (Ms dx) out."""
+
+    def __init__(self, xdim, ydim, zdim, batch=1):
+        self.shape = (zdim, ydim, xdim)
+        self.batch = batch
+        h = _VP()
+        _check(load().mms_sno_create(xdim, ydim, zdim, batch, ctypes.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def num_params():
+        return int(load().mms_sno_num_params())
+
+    def close(self):
+        if self.h:
+            load().mms_sno_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        _check(load().mms_sno_set_weights(self.h, _ptr(w), w.size))
+
+    def get_weights(self, bf16_rounded=False):
+        w = np.empty(self.num_params(), np.float32)
+        _check(load().mms_sno_get_weights(self.h, _ptr(w), w.size, int(bf16_rounded)))
+        return w
+
+    def forward_dev(self, u, out, nbatch=1):
+        _check(load().mms_sno_forward_dev(self.h, _ptr(u), _ptr(out), nbatch))
+
+    def gradient(self, u, far, nbatch=1):
+        g = np.empty(self.num_params(), np.float32)
+        loss = ctypes.c_double()
+        _check(load().mms_sno_gradient(self.h, _ptr(u), _ptr(far), nbatch, _ptr(g), ctypes.byref(loss)))
+        return loss.value, g
+
+    def train_step(self, u, far, nbatch, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+        loss = ctypes.c_double()
+        _check(load().mms_sno_train_step(self.h, _ptr(u), _ptr(far), nbatch, lr, beta1, beta2, eps,
+                                         ctypes.byref(loss)))
+        return loss.value
+
+    def device_bytes(self):
+        return int(load().mms_sno_device_bytes(self.h))
+
