@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--dt", type=float, default=1e-13)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the learned far-field measurement")
     ap.add_argument("--workload", choices=["single", "ensemble"], default="single",
                     help="single: the 256x256x3 metric; ensemble: the batched-ensemble configuration")
     ap.add_argument("--ensemble-size", type=int, default=512)
@@ -355,6 +356,10 @@ def run_ours(args):
                "d2h_bytes_per_step": int(out_M.numel() * 8),
                "path": "mms_state_set_dev + mms_run_fixed(1 step) + mms_state_get_dev, pinned host copies"}
 
+    sur = None
+    if args.solver == "fmm" and not args.no_surrogate:
+        sur = surrogate_block(args, grid, params, mask, M, stream, flush, value)
+
     base = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -382,6 +387,8 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": cfg,
             "cell_steps_per_s": value * N, "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
             "e2e": e2e, "cpu_baseline": base}
+    if sur is not None:
+        line["surrogate"] = sur
     if acc is not None:
         line["accuracy"] = {"demag_phi_rel_l2_vs_direct": acc,
                             "note": "direct = exact FP32 table + compensated sum, itself <= 2e-6 from FP64"}
@@ -391,6 +398,63 @@ def run_ours(args):
 
 STAGE_KERNEL = {"p2m": "k_p2m_row", "m2m": "k_m2m_c (one launch per level)", "m2l": "k_m2l_res / k_m2l_split",
                 "l2l": "k_l2l_c (one launch per level)", "l2p_p2p": "k_p2p + k_l2p"}
+
+
+def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
+    """The learned far field on the same workload: its demag error on the start
+    state against the exact sum, LLG steps/s with the surrogate alone (no
+    check), and the surrogate-assisted run the metric names (FMM check every
+    50 steps, 1e-3 rel-L2 tolerance, FMM takes over above it)."""
+    import torch
+    import mmsb200
+    from mmsb200 import surrogate as S
+    w, meta = S.load_weights()
+    if w is None:
+        return {"unavailable": "no trained weights (python -m mmsb200.surrogate)"}
+    X, Y, Z = grid.xdim, grid.ydim, grid.zdim
+    solver = mmsb200.make_solver(mmsb200.SOLVER_SURROGATE, 4, 4)
+    out = {"network": "3-D conv U-Net on 4x4 leaf patches, 4 levels, 32 channels, %d BF16 weights, FP32 accumulation"
+           % mmsb200.SNO.num_params(),
+           "training": {k: (float(v) if np.ndim(v) == 0 else v.tolist()) for k, v in meta.items()},
+           "inference": "BF16 activations (fast mode)"}
+    Mf = torch.from_numpy(M.astype(np.float32)).cuda()
+    rho = torch.empty((Z, Y, X), dtype=torch.float32, device="cuda")
+    phi_s, phi_d = torch.empty_like(rho), torch.empty_like(rho)
+    with mmsb200.Context(grid, params, solver, stream=stream.cuda_stream) as c:
+        c.set_surrogate(w, 0, 1.0)
+        c.divergence_dev(Mf, rho)
+        c.potential_dev(rho, phi_s)
+        with mmsb200.Context(grid, params, mmsb200.make_solver(mmsb200.SOLVER_DIRECT),
+                             stream=stream.cuda_stream) as dctx:
+            dctx.potential_dev(rho, phi_d)
+            dctx.sync()
+        out["demag_phi_rel_l2_vs_direct"] = float((phi_s.double() - phi_d.double()).norm() / phi_d.double().norm())
+
+    def steps_per_s(every, tol, nsteps):
+        with mmsb200.Context(grid, params, solver, stream=stream.cuda_stream) as c:
+            c.set_surrogate(w, every, tol)
+            c.state_set(mask, M)
+            c.run_fixed(args.dt, 3)
+            c.sync()
+            st0 = c.surrogate_stats()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.fill_(0.0)
+            e0.record(stream)
+            c.run_fixed(args.dt, nsteps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            st = c.surrogate_stats()
+            st["checks"] -= st0["checks"]
+            return nsteps / (e0.elapsed_time(e1) * 1e-3), st
+
+    v, _ = steps_per_s(0, 1.0, 200)
+    out["steps_per_s_surrogate_only"] = v
+    out["speedup_surrogate_only_vs_fmm"] = v / fmm_value
+    v, st = steps_per_s(50, 1e-3, 200)
+    out["assisted_check50_tol1e-3"] = {"steps_per_s": v, "checks": st["checks"], "fallbacks": st["fallbacks"],
+                                       "first_check_rel_l2_vs_fmm": st["max_err"],
+                                       "surrogate_active_at_end": st["active"]}
+    return out
 
 
 def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):

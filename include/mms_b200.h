@@ -279,9 +279,11 @@ long long mms_sno_device_bytes(const mms_sno *net);
  * every `check_every` accepted steps plus every rejected step of mms_march,
  * the potential of the current state is computed by both the surrogate and
  * the FMM (the solver's order, leaf 4); when their rel-L2 difference exceeds
- * `tol` the FMM replaces the surrogate for the rest of the run.  Cubic cells
- * only. */
-int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol);
+ * `tol` the FMM replaces the surrogate for the rest of the run.  fast != 0:
+ * the network runs on BF16 activations (hi products only: half the tensor-core
+ * work, ~1e-3 relative rounding of the far field) instead of hi/lo pairs.
+ * Cubic cells only. */
+int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol, int fast);
 /* runs that check now on the current state; *err = rel-L2(surrogate, FMM) */
 int mms_surrogate_check(mms_ctx *ctx, double *err);
 /* active: 1 while the surrogate is in use, 0 after the FMM took over */

@@ -846,7 +846,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
 
 // ---- surrogate solver ------------------------------------------------------------
 
-int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol)
+int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol, int fast)
 {
     if (!ctx || !w || check_every < 0 || !(tol > 0)) {
         mms_set_error("mms_ctx_set_surrogate: bad argument");
@@ -866,6 +866,7 @@ int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int che
         ctx->dev_bytes += (size_t)mms_sno_device_bytes(ctx->sno);
     }
     MMS_TRY(mms_sno_set_weights(ctx->sno, w, count));
+    sno_set_fast(ctx->sno, fast != 0);
     ctx->sur_every = check_every;
     ctx->sur_tol = tol;
     ctx->sur_active = true;

@@ -148,6 +148,7 @@ int launch_potential_split(mms_ctx *ctx, const float *rho, float *phi, float *ne
 int sno_launch_far(mms_sno *n, cudaStream_t st, const float *rho, float in_scale, float *phi, const float *near,
                    float out_scale, cudaEvent_t wait_before_head, int64_t *launches);
 int sno_error_flag(mms_sno *n, cudaStream_t st);
+void sno_set_fast(mms_sno *n, bool fast);
 // rel-L2 |a - b| / |b| over n floats (tune.cu); synchronises ctx->stream
 int rel_l2_dev(mms_ctx *ctx, const float *a, const float *b, long long n, double *out);
 void fmm_plan_destroy(mms_ctx *ctx);

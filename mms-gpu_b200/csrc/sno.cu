@@ -56,9 +56,10 @@ constexpr int PATCH = 4;
 constexpr int CH = 32;
 constexpr int LEVELS = 4;
 constexpr int CIN0 = PATCH * PATCH;
-constexpr int CS = 4;    // pipeline stages of k_conv
 constexpr int CBN = 32;  // output channels per tile (N of the MMA)
-constexpr int CONV_SMEM = CS * (umma::BM * 128) + CS * (CBN * 128) + 1024 + 128;
+// pipeline stages of k_conv: 4 for training (2 CTAs per SM over many tiles),
+// 8 for the solver's batch-1 inference (few tiles: depth hides the latency)
+constexpr int conv_smem(int stages) { return stages * (umma::BM * 128) + stages * (CBN * 128) + 1024 + 128; }
 
 struct Layer {
     int pat, cin, cout, in, out, skip, taps;
@@ -126,8 +127,8 @@ struct ConvP {
     int cin_log2, T, pat;
     int Z, Hin, Win, Hout, Wout;
     int P;                  // output rows
-    const bf16 *w;          // [N][K], K = 2 T cin: [W | W] for the hi and lo halves
-    int K, N;
+    const bf16 *w;          // [N][ldw], ldw = 2 T cin: [W | W] for the hi and lo halves
+    int K, N, ldw;          // K = ldw (hi and lo) or T cin (hi only)
     int ep;
     const bf16 *shi, *slo;  // EP_SPLIT: skip tensor added before the split (may be NULL)
     bf16 *ohi, *olo;        // EP_SPLIT outputs [P][N]
@@ -165,6 +166,7 @@ __device__ __forceinline__ bool tap_src(const ConvP &p, int tap, int bz, int z, 
     }
 }
 
+template <int CS>
 __global__ void __launch_bounds__(128) k_conv(ConvP p)
 {
     extern __shared__ uint8_t smraw[];
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(128) k_conv(ConvP p)
             const int gk = kt * umma::BK + cc * 8;
             const bool ok = r < p.N && gk < p.K;
             umma::cp_async16(sb_st + umma::sw128_off(r, cc),
-                             ok ? (const void *)(p.w + (long long)r * p.K + gk) : (const void *)p.w, ok);
+                             ok ? (const void *)(p.w + (long long)r * p.ldw + gk) : (const void *)p.w, ok);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
@@ -249,7 +251,15 @@ __global__ void __launch_bounds__(128) k_conv(ConvP p)
     for (int kt = 0; kt < nk && ok; kt++) {
         const int st = kt % CS;
         const int pending = issued - kt - 1;  // groups allowed to stay in flight
-        if (pending >= 2)
+        if (pending >= 6)
+            asm volatile("cp.async.wait_group 6;\n" ::: "memory");
+        else if (pending == 5)
+            asm volatile("cp.async.wait_group 5;\n" ::: "memory");
+        else if (pending == 4)
+            asm volatile("cp.async.wait_group 4;\n" ::: "memory");
+        else if (pending == 3)
+            asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+        else if (pending == 2)
             asm volatile("cp.async.wait_group 2;\n" ::: "memory");
         else if (pending == 1)
             asm volatile("cp.async.wait_group 1;\n" ::: "memory");
@@ -594,6 +604,7 @@ struct mms_sno {
     double *lsum = nullptr, *h_lsum = nullptr;
     int *err = nullptr;
     int adam_t = 0;
+    bool fast = false;  // solver inference: BF16 activations (hi products only)
     size_t bytes = 0;
     std::vector<void *> allocs;
 
@@ -620,13 +631,12 @@ int sno_alloc(mms_sno *n, T **p, size_t count)
 
 int conv_attr_once()
 {
-    static int done = -1;
     static int dev_done = -1;
     int dev = 0;
     cudaGetDevice(&dev);
-    if (done == 0 && dev_done == dev) return MMS_OK;
-    MMS_CUDA_TRY(cudaFuncSetAttribute(k_conv, cudaFuncAttributeMaxDynamicSharedMemorySize, CONV_SMEM));
-    done = 0;
+    if (dev_done == dev) return MMS_OK;
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_conv<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem(4)));
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_conv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, conv_smem(8)));
     dev_done = dev;
     return MMS_OK;
 }
@@ -650,7 +660,7 @@ ConvP conv_params(const mms_sno *n, const Layer &y, int nb, bool adjoint)
         p.Wout = n->W[lout];
         p.P = (int)n->rows(lout, nb);
         p.w = n->wf + y.wf_off;
-        p.K = 2 * y.taps * y.cin;
+        p.K = p.ldw = 2 * y.taps * y.cin;
         p.N = y.cout;
     } else {
         // gradient w.r.t. the layer input: the adjoint pattern over the input rows
@@ -665,22 +675,28 @@ ConvP conv_params(const mms_sno *n, const Layer &y, int nb, bool adjoint)
         p.Wout = n->W[lin];
         p.P = (int)n->rows(lin, nb);
         p.w = n->wb + y.wb_off;
-        p.K = 2 * y.taps * y.cout;
+        p.K = p.ldw = 2 * y.taps * y.cout;
         p.N = y.cin;
     }
     return p;
 }
 
-int launch_conv(const ConvP &p, cudaStream_t st)
+// fast: batch-1 inference, hi products only (BF16 activations) and a deep pipeline
+int launch_conv(ConvP p, cudaStream_t st, bool fast = false)
 {
     MMS_TRY(conv_attr_once());
-    k_conv<<<div_up(p.P, umma::BM), 128, CONV_SMEM, st>>>(p);
+    if (fast) {
+        p.K = p.ldw / 2;
+        k_conv<8><<<div_up(p.P, umma::BM), 128, conv_smem(8), st>>>(p);
+    } else {
+        k_conv<4><<<div_up(p.P, umma::BM), 128, conv_smem(4), st>>>(p);
+    }
     MMS_CUDA_TRY(cudaGetLastError());
     return MMS_OK;
 }
 
 // forward through every layer except the head; the head is issued by the caller
-int forward_body(mms_sno *n, int nb, const float *u, float uscale, cudaStream_t st)
+int forward_body(mms_sno *n, int nb, const float *u, float uscale, cudaStream_t st, bool fast = false)
 {
     const long long P0 = n->rows(0, nb);
     k_patchify<<<div_up(P0 * CIN0, 256), 256, 0, st>>>(u, uscale, n->X, n->Y, n->H[0], n->W[0], P0, n->ahi[0],
@@ -696,7 +712,7 @@ int forward_body(mms_sno *n, int nb, const float *u, float uscale, cudaStream_t 
             p.shi = n->ahi[y.skip];
             p.slo = n->alo[y.skip];
         }
-        MMS_TRY(launch_conv(p, st));
+        MMS_TRY(launch_conv(p, st, fast));
     }
     return MMS_OK;
 }
@@ -834,7 +850,7 @@ int loss_and_grad(mms_sno *n, int nb, const float *u, const float *far, float us
 int sno_launch_far(mms_sno *n, cudaStream_t st, const float *rho, float in_scale, float *phi, const float *near,
                    float out_scale, cudaEvent_t wait_before_head, int64_t *launches)
 {
-    MMS_TRY(forward_body(n, 1, rho, in_scale, st));
+    MMS_TRY(forward_body(n, 1, rho, in_scale, st, n->fast));
     if (wait_before_head) MMS_CUDA_TRY(cudaStreamWaitEvent(st, wait_before_head, 0));
     ConvP ph = conv_params(n, n->L.back(), 1, false);
     ph.ep = EP_PHI;
@@ -843,12 +859,14 @@ int sno_launch_far(mms_sno *n, cudaStream_t st, const float *rho, float in_scale
     ph.scale = out_scale;
     ph.X = n->X;
     ph.Y = n->Y;
-    MMS_TRY(launch_conv(ph, st));
+    MMS_TRY(launch_conv(ph, st, n->fast));
     if (launches) *launches += (int64_t)n->L.size() + 1;
     return MMS_OK;
 }
 
 int sno_error_flag(mms_sno *n, cudaStream_t st) { return check_err(n, st); }
+
+void sno_set_fast(mms_sno *n, bool fast) { n->fast = fast; }
 
 // ---------------------------------------------------------------------------
 // C ABI

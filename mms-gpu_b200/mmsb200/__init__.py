@@ -128,7 +128,7 @@ SIGNATURES = {
     "mms_sno_train_step": (_I, [_VP, _VP, _VP, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                 ctypes.POINTER(_D)]),
     "mms_sno_device_bytes": (ctypes.c_longlong, [_VP]),
-    "mms_ctx_set_surrogate": (_I, [_VP, _VP, ctypes.c_longlong, _I, _D]),
+    "mms_ctx_set_surrogate": (_I, [_VP, _VP, ctypes.c_longlong, _I, _D, _I]),
     "mms_surrogate_check": (_I, [_VP, ctypes.POINTER(_D)]),
     "mms_surrogate_stats": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
@@ -309,9 +309,9 @@ class Context:
         """FMM potential and its exact near-field part (device arrays)"""
         _check(load().mms_potential_split_dev(self.h, _ptr(rho), _ptr(phi), _ptr(near)))
 
-    def set_surrogate(self, weights, check_every=50, tol=1e-3):
+    def set_surrogate(self, weights, check_every=50, tol=1e-3, fast=True):
         w = np.ascontiguousarray(weights, np.float32)
-        _check(load().mms_ctx_set_surrogate(self.h, _ptr(w), w.size, check_every, tol))
+        _check(load().mms_ctx_set_surrogate(self.h, _ptr(w), w.size, check_every, tol, int(fast)))
 
     def surrogate_check(self):
         e = ctypes.c_double()

@@ -1,0 +1,303 @@
+"""Training and use of the surrogate far-field network (mms_sno).
+
+Training pairs are (u, far) = (rho dx / Ms, (phi_FMM - phi_near) / (Ms dx))
+taken along LLG trajectories that the library itself integrates: instances of
+64..256 cells a side (disc lattices, discs, ellipses, rectangles, block-masked
+films; in-plane, per-dot, vortex or random initial states; constant or ramped
+in-plane fields up to 50 mT) placed in a fixed canvas, stepped with the FMM,
+and evaluated every few steps by a high-order FMM (P = 8, leaf 4) whose exact
+near field (mms_potential_split_dev) is subtracted.  The network is then fitted
+by the library's own forward / backward / Adam kernels (mms_sno_train_step).
+
+Everything here runs through the C ABI; torch only holds device buffers.
+"""
+from __future__ import annotations
+
+import math
+import os
+import time
+
+import numpy as np
+
+from . import (SNO, SOLVER_FMM, Context, Grid, geometry, make_params, make_solver)
+
+MS = geometry.MS_PERMALLOY
+DX = 5e-9
+WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "sno_patch4_c32_l4.npz")
+
+
+# ---- training geometries ------------------------------------------------------
+
+def _instance(rng, Z):
+    """(mask, M) of one instance with sides drawn from 64..256"""
+    sides = (64, 96, 128, 160, 192, 224, 256)
+    sx, sy = int(rng.choice(sides)), int(rng.choice(sides))
+    kind = int(rng.integers(0, 6))
+    seed = int(rng.integers(0, 2 ** 31))
+    if kind in (0, 1):  # disc lattice (the benchmark's family)
+        r = int(rng.integers(5, 17))
+        pitch = 2 * r + int(rng.integers(2, 14))
+        if kind == 0:
+            mask, M = geometry.per_dot_random_inplane(sx, sy, Z, r, pitch, seed)
+        else:
+            mask = geometry.disc_lattice(sx, sy, Z, r, pitch)
+            M = geometry.random_sphere(mask, seed)
+    elif kind == 2:  # one disc or ellipse
+        ax = rng.uniform(0.25, 0.5) * (sx - 2)
+        ay = rng.uniform(0.25, 0.5) * (sy - 2)
+        mask = geometry.from_plane(geometry.ellipse_plane(sx, sy, (sx - 1) / 2, (sy - 1) / 2, ax, ay), Z)
+        M = geometry.vortex(mask, 2.0, 10.0, seed) if rng.uniform() < 0.5 else geometry.random_inplane(mask, seed)
+    elif kind == 3:  # rectangle
+        mask = geometry.reference_default(sx, sy, Z)
+        M = geometry.single_domain(mask, phi=rng.uniform(0, 2 * np.pi)) if rng.uniform() < 0.3 else \
+            geometry.random_inplane(mask, seed)
+    elif kind == 4:  # block-masked film
+        mask = geometry.random_blocks_mask(sx, sy, Z, rng.uniform(0.1, 0.5), 4, seed)
+        M = geometry.random_sphere(mask, seed + 1)
+    else:  # vortex-quadrant square
+        mask = geometry.reference_default(sx, sy, Z)
+        M = geometry.vortex_quadrants(mask)
+    return mask, M
+
+
+def _place(mask, M, X, Y, rng):
+    Z, sy, sx = mask.shape
+    ox, oy = int(rng.integers(0, X - sx + 1)), int(rng.integers(0, Y - sy + 1))
+    m = np.zeros((Z, Y, X), np.uint8)
+    v = np.zeros((Z, Y, X, 3))
+    m[:, oy:oy + sy, ox:ox + sx] = mask
+    v[:, oy:oy + sy, ox:ox + sx] = M
+    return m, v
+
+
+def _field(rng):
+    """external field table: constant or a 10 ns ramp along a random in-plane direction"""
+    ph = rng.uniform(0, 2 * np.pi)
+    d = np.array([np.cos(ph), np.sin(ph), 0.0])
+    if rng.uniform() < 0.5:
+        b = 0.05 * math.sqrt(rng.uniform())
+        return [0.0], [list(b * d)]
+    return [0.0, 1e-8], [list(-0.05 * d), list(0.05 * d)]
+
+
+def generate_pairs(n_pairs, X=256, Y=256, Z=3, snaps_per_run=50, steps_between=10, dt=1e-13, seed=2010,
+                   target_order=8, progress=None):
+    """n_pairs training pairs as two torch tensors [n, Z, Y, X] (float32, cuda)"""
+    import torch
+    rng = np.random.Generator(np.random.Philox(seed))
+    N = X * Y * Z
+    U = torch.empty((n_pairs, Z, Y, X), dtype=torch.float32, device="cuda")
+    F = torch.empty_like(U)
+    grid = Grid(X, Y, Z, DX, DX, DX)
+    dyn = Context(grid, make_params(), make_solver(SOLVER_FMM, 4, 4))
+    tgt = Context(grid, make_params(), make_solver(SOLVER_FMM, target_order, 4))
+    Mdev = torch.empty((N, 3), dtype=torch.float64, device="cuda")
+    rho = torch.empty(N, dtype=torch.float32, device="cuda")
+    phi = torch.empty_like(rho)
+    near = torch.empty_like(rho)
+    k = 0
+    t0 = time.time()
+    try:
+        while k < n_pairs:
+            mask, M = _place(*_instance(rng, Z), X, Y, rng)
+            ht, hb = _field(rng)
+            dyn.set_params(make_params(external=True, hext_t=ht, hext_b=hb))
+            dyn.state_set(mask, M)
+            for s in range(snaps_per_run):
+                if k >= n_pairs:
+                    break
+                if s:
+                    dyn.run_fixed(dt, steps_between)
+                dyn.state_get_dev(Mdev)
+                dyn.divergence_dev(Mdev.float(), rho)
+                tgt.potential_split_dev(rho, phi, near)
+                U[k] = (rho * (DX / MS)).view(Z, Y, X)
+                F[k] = ((phi - near) / (MS * DX)).view(Z, Y, X)
+                k += 1
+            if progress:
+                progress(k, time.time() - t0)
+        torch.cuda.synchronize()
+    finally:
+        dyn.close()
+        tgt.close()
+    return U, F
+
+
+def benchmark_pairs(n_pairs, seed=777, X=256, Y=256, Z=3, steps_between=20, dt=1e-13):
+    """held-out pairs of the benchmark workload itself (8 x 8 disc lattice,
+    r = 12, pitch 32, per-dot random in-plane M, B_x ramp -50..+50 mT / 10 ns),
+    seeds disjoint from training"""
+    import torch
+    grid = Grid(X, Y, Z, DX, DX, DX)
+    N = X * Y * Z
+    U = torch.empty((n_pairs, Z, Y, X), dtype=torch.float32, device="cuda")
+    F = torch.empty_like(U)
+    P = torch.empty_like(U)
+    Mdev = torch.empty((N, 3), dtype=torch.float64, device="cuda")
+    rho = torch.empty(N, dtype=torch.float32, device="cuda")
+    phi = torch.empty_like(rho)
+    near = torch.empty_like(rho)
+    prm = make_params(external=True, hext_t=[0.0, 1e-8], hext_b=[[-0.05, 0, 0], [0.05, 0, 0]])
+    with Context(grid, prm, make_solver(SOLVER_FMM, 4, 4)) as dyn, \
+            Context(grid, make_params(), make_solver(SOLVER_FMM, 8, 4)) as tgt:
+        per_run = 10
+        for k in range(n_pairs):
+            if k % per_run == 0:
+                mask, M = geometry.per_dot_random_inplane(X, Y, Z, 12, 32, seed + k)
+                dyn.state_set(mask, M)
+            else:
+                dyn.run_fixed(dt, steps_between)
+            dyn.state_get_dev(Mdev)
+            dyn.divergence_dev(Mdev.float(), rho)
+            tgt.potential_split_dev(rho, phi, near)
+            U[k] = (rho * (DX / MS)).view(Z, Y, X)
+            F[k] = ((phi - near) / (MS * DX)).view(Z, Y, X)
+            P[k] = (phi / (MS * DX)).view(Z, Y, X)
+    return U, F, P
+
+
+# ---- training -------------------------------------------------------------------
+
+def layer_shapes():
+    """(kind, taps, cin, cout) of every layer in weight order: conv3 x -> a0;
+    per level 1..3 down + conv3; bottleneck conv3; per level 2..0 up + conv3;
+    point head (the library's network, mms_sno)"""
+    L = [("conv3", 27, 16, 32)]
+    for _ in range(3):
+        L += [("down", 4, 32, 32), ("conv3", 27, 32, 32)]
+    L.append(("conv3", 27, 32, 32))
+    for _ in range(3):
+        L += [("up", 4, 32, 32), ("conv3", 27, 32, 32)]
+    L.append(("point", 1, 32, 16))
+    return L
+
+
+def init_weights(seed=1):
+    """per-layer uniform +-sqrt(3 / fan_in), seeded Philox; fan_in = taps x cin
+    (cin for an up transfer, where each output takes one tap)"""
+    g = np.random.Generator(np.random.Philox(seed))
+    parts = []
+    for kind, taps, cin, cout in layer_shapes():
+        fan_in = cin if kind == "up" else taps * cin
+        lim = np.sqrt(3.0 / fan_in)
+        parts.append(g.uniform(-lim, lim, cout * taps * cin))
+    w = np.concatenate(parts).astype(np.float32)
+    assert w.size == SNO.num_params()
+    return w
+
+
+def evaluate(net, U, F, P=None, batch=8):
+    """mean and max rel-L2 of the network's far field (and of the total
+    potential when P, the full potential, is given) over the pairs"""
+    import torch
+    out = torch.empty((batch,) + tuple(U.shape[1:]), dtype=torch.float32, device="cuda")
+    ef, et = [], []
+    for i in range(0, U.shape[0], batch):
+        nb = min(batch, U.shape[0] - i)
+        net.forward_dev(U[i:i + nb], out, nb)
+        d = (out[:nb] - F[i:i + nb]).double()
+        ef += (d.flatten(1).norm(dim=1) / F[i:i + nb].double().flatten(1).norm(dim=1)).tolist()
+        if P is not None:
+            et += (d.flatten(1).norm(dim=1) / P[i:i + nb].double().flatten(1).norm(dim=1)).tolist()
+    r = dict(far_mean=float(np.mean(ef)), far_max=float(np.max(ef)))
+    if P is not None:
+        r.update(total_mean=float(np.mean(et)), total_max=float(np.max(et)))
+    return r
+
+
+def train(U, F, steps, batch=8, lr_max=2e-3, lr_min=1e-5, warmup=0.03, seed=1, weights=None, val=None,
+          log_every=500, log=print):
+    """fits a fresh (or the given) network to the pairs with Adam on a
+    warm-up + cosine schedule; returns (weights, history)"""
+    import torch
+    Z, Y, X = U.shape[1:]
+    net = SNO(X, Y, Z, batch)
+    net.set_weights(init_weights(seed) if weights is None else weights)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    hist = []
+    t0 = time.time()
+    n = U.shape[0]
+    perm = torch.randperm(n, generator=g)
+    pos = 0
+    ub = torch.empty((batch, Z, Y, X), dtype=torch.float32, device="cuda")
+    fb = torch.empty_like(ub)
+    for it in range(steps):
+        if pos + batch > n:
+            perm = torch.randperm(n, generator=g)
+            pos = 0
+        idx = perm[pos:pos + batch].cuda()
+        pos += batch
+        torch.index_select(U, 0, idx, out=ub)
+        torch.index_select(F, 0, idx, out=fb)
+        w = it / max(1, steps - 1)
+        if w < warmup:
+            lr = lr_max * (it + 1) / (warmup * steps)
+        else:
+            lr = lr_min + 0.5 * (lr_max - lr_min) * (1 + math.cos(math.pi * (w - warmup) / (1 - warmup)))
+        loss = net.train_step(ub, fb, batch, lr)
+        if it % log_every == 0 or it == steps - 1:
+            rec = dict(step=it, loss=loss, lr=lr, s=time.time() - t0)
+            if val is not None:
+                rec.update(evaluate(net, *val))
+            hist.append(rec)
+            if log:
+                log(rec)
+    w = net.get_weights()
+    net.close()
+    return w, hist
+
+
+def save_weights(path, w, meta):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez_compressed(path, weights=np.asarray(w, np.float32), **{k: np.asarray(v) for k, v in meta.items()})
+
+
+def load_weights(path=DEFAULT_WEIGHTS):
+    """(weights, meta) or (None, None) when the file is absent"""
+    if not os.path.exists(path):
+        return None, None
+    with np.load(path) as z:
+        meta = {k: z[k] for k in z.files if k != "weights"}
+        return z["weights"].astype(np.float32), meta
+
+
+def main(argv=None):
+    import argparse
+    import json
+
+    import torch
+    ap = argparse.ArgumentParser(description="train the surrogate far-field network")
+    ap.add_argument("--pairs", type=int, default=20000)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--val", type=int, default=100)
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--log", default=None)
+    a = ap.parse_args(argv)
+    logf = open(a.log, "w") if a.log else None
+
+    def log(rec):
+        line = json.dumps(rec)
+        print(line, flush=True)
+        if logf:
+            logf.write(line + "\n")
+            logf.flush()
+
+    t0 = time.time()
+    U, F = generate_pairs(a.pairs, progress=lambda k, s: k % 2000 < 50 and log(dict(pairs=k, s=round(s, 1))))
+    log(dict(generated=a.pairs, s=time.time() - t0))
+    val = benchmark_pairs(a.val)
+    w, hist = train(U, F, a.steps, a.batch, a.lr, val=val, log=log)
+    del U, F
+    torch.cuda.empty_cache()
+    final = hist[-1]
+    save_weights(a.out, w, dict(pairs=a.pairs, steps=a.steps, batch=a.batch, lr=a.lr, patch=4, channels=32,
+                                levels=4, val_far_mean=final.get("far_mean", -1),
+                                val_total_mean=final.get("total_mean", -1)))
+    log(dict(saved=a.out, total_s=time.time() - t0))
+
+
+if __name__ == "__main__":
+    main()

@@ -80,17 +80,19 @@ def test_training_fits_a_fixed_linear_map(cuda, lib):
     assert np.mean(losses[-10:]) < 0.05 * np.mean(losses[:5]), (losses[:5], losses[-10:])
 
 
-def _surrogate_ctx(mmsb200, mask, M, w, every, tol, order=4):
+def _surrogate_ctx(mmsb200, mask, M, w, every, tol, order=4, fast=True):
     Z, Y, X = mask.shape
     ctx = mmsb200.Context(mmsb200.Grid(X, Y, Z, 5e-9, 5e-9, 5e-9), mmsb200.make_params(),
                           mmsb200.make_solver(mmsb200.SOLVER_SURROGATE, order, 4))
-    ctx.set_surrogate(w, every, tol)
+    ctx.set_surrogate(w, every, tol, fast)
     ctx.state_set(mask, M)
     return ctx
 
 
-def test_surrogate_potential_is_near_plus_network(cuda, lib):
-    """phi(surrogate) = exact near field + (Ms dx) net(rho dx / Ms)"""
+@pytest.mark.parametrize("fast", [False, True])
+def test_surrogate_potential_is_near_plus_network(cuda, lib, fast):
+    """phi(surrogate) = exact near field + (Ms dx) net(rho dx / Ms); the fast
+    mode rounds the activations to BF16"""
     import torch
     import mmsb200
     from mmsb200 import geometry
@@ -107,13 +109,17 @@ def test_surrogate_potential_is_near_plus_network(cuda, lib):
         phi = torch.zeros_like(rho)
         near = torch.zeros_like(rho)
         fctx.potential_split_dev(rho, phi, near)
-    with _surrogate_ctx(mmsb200, mask, M, w, 0, 1.0) as ctx:
+    with _surrogate_ctx(mmsb200, mask, M, w, 0, 1.0, fast=fast) as ctx:
         ps = torch.zeros_like(rho)
         ctx.potential_dev(rho, ps)
         torch.cuda.synchronize()
     u = (rho.cpu().numpy() * dx / Ms).reshape(1, 3, 48, 64).astype(np.float64)
-    ref = near.cpu().numpy() + Ms * dx * sno.far_field(sno.round_bf16(w).astype(np.float64), u).ravel()
-    assert rel_l2(ps.cpu().numpy(), ref) < 1e-5
+    far = Ms * dx * sno.far_field(sno.round_bf16(w).astype(np.float64), u).ravel()
+    ref = near.cpu().numpy() + far
+    if fast:
+        assert rel_l2(ps.cpu().numpy() - near.cpu().numpy(), far) < 1e-2
+    else:
+        assert rel_l2(ps.cpu().numpy(), ref) < 1e-5
 
 
 def test_check_falls_back_to_fmm(cuda, lib):
@@ -154,3 +160,38 @@ def test_check_keeps_a_passing_surrogate(cuda, lib):
         st = ctx.surrogate_stats()
         assert st["checks"] == 3 and st["fallbacks"] == 0 and st["active"]
         assert abs(ctx.surrogate_check() - st["last_err"]) < 0.5 * st["last_err"] + 1e-9
+
+
+def test_trained_network_gain_over_near_field_only(cuda, lib):
+    """What the trained network adds: on a held-out state of the benchmark
+    workload (8 x 8 disc lattice, per-dot random in-plane M, seed outside the
+    training set), the potential from the exact near field alone misses the
+    far field entirely; near field + network recovers it to a few percent of
+    the exact (direct-sum) potential."""
+    import torch
+    import mmsb200
+    from mmsb200 import geometry, surrogate
+    w, meta = surrogate.load_weights()
+    assert w is not None, "trained weights missing"
+    mask, M = geometry.per_dot_random_inplane(256, 256, 3, 12, 32, 4242)
+    grid = mmsb200.Grid(256, 256, 3, 5e-9, 5e-9, 5e-9)
+    rho = torch.zeros(3 * 256 * 256, device="cuda")
+    exact, ps, phi, near = (torch.zeros_like(rho) for _ in range(4))
+    with mmsb200.Context(grid, mmsb200.make_params(), mmsb200.make_solver(mmsb200.SOLVER_DIRECT)) as d:
+        d.divergence_dev(torch.from_numpy(M.astype(np.float32)).cuda(), rho)
+        d.potential_dev(rho, exact)
+        d.sync()
+    with mmsb200.Context(grid, mmsb200.make_params(), mmsb200.make_solver(mmsb200.SOLVER_FMM, 4, 4)) as f:
+        f.potential_split_dev(rho, phi, near)
+        f.sync()
+    with _surrogate_ctx(mmsb200, mask, M, w, 0, 1.0) as s:
+        s.potential_dev(rho, ps)
+        s.sync()
+    ex = exact.double()
+    e_near = float((near.double() - ex).norm() / ex.norm())
+    e_sur = float((ps.double() - ex).norm() / ex.norm())
+    e_fmm = float((phi.double() - ex).norm() / ex.norm())
+    assert e_near > 0.2            # the far field is a large part of phi here
+    assert e_sur < 0.1 * e_near    # the network recovers > 90 % of it
+    assert e_sur < 0.05
+    assert e_fmm < 1e-3            # the check's reference is within the target
