@@ -90,7 +90,11 @@ typedef struct {
     int fmm_leaf;            /* leaf box side in cells (FMM), 2..16, or 0=auto */
     int m2l_mode;            /* FMM M2L: 0 auto, 1 FP32 SIMT, 2 tensor cores
                                 (tcgen05, split-BF16 hi/lo products)          */
-    int reserved[4];
+    int far_mode;            /* FMM far field: 0 one launch per stage and
+                                level (default, fastest measured), 1 P2M ..
+                                L2L in one cooperative launch with grid
+                                barriers (P <= 4, FP32 M2L); identical bits   */
+    int reserved[3];
 } mms_solver;
 
 typedef struct mms_ctx mms_ctx;
@@ -244,6 +248,14 @@ int mms_potential_direct_noalloc(const float *rho, float *phi, int xdim, int ydi
  * counterpart (the reference hard-codes P, main.cpp:31). */
 int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, const float *rho_dev, double max_rel_err,
                      int reps, mms_solver *best, double *best_ms, double *best_err);
+/* Same search, timed on what a time-stepping caller runs: each candidate
+ * within the error target starts from the host state (material, M as
+ * mms_state_set takes them) and *best_ms is its mean graph-captured RK4 step
+ * of size dt over `reps` steps.  rho_dev is the charge density of that state
+ * (the error sample). */
+int mms_autotune_fmm_steps(const mms_grid *grid, const mms_params *params, const uint8_t *material,
+                           const double *M, double dt, const float *rho_dev, double max_rel_err, int reps,
+                           mms_solver *best, double *best_ms, double *best_err);
 
 /* surrogate far field ---------------------------------------------------------
  * A 3-D convolutional neural operator (U-Net over the 4 x 4-cell patch grid,

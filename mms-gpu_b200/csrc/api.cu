@@ -6,6 +6,7 @@
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -288,6 +289,15 @@ int clear_numeric_flag(mms_ctx *ctx)
 
 }  // namespace
 
+bool pdl_enabled()
+{
+    static const bool on = [] {
+        const char *e = getenv("MMS_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 int launch_potential(mms_ctx *ctx, const float *rho, float *phi)
 {
     if (ctx->s.kind == MMS_SOLVER_SURROGATE)
@@ -458,6 +468,10 @@ int mms_ctx_sync(mms_ctx *ctx)
         return MMS_ERR_ARG;
     }
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (fmm_far_error(ctx)) {
+        mms_set_error("FMM far field: a grid barrier wait timed out");
+        return MMS_ERR_CUDA;
+    }
     return MMS_OK;
 }
 

@@ -20,6 +20,7 @@
 // are FP32 real vectors of the (re, im) pairs for m >= 0, even n + m first;
 // M2M, M2L and L2L act on the two parity blocks separately.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -55,6 +56,8 @@ struct TcGroup {
 
 }  // namespace
 
+struct FarSync;
+
 struct FmmPlan {
     FmmDev d{};
     int KPb[2] = {0, 0};      // padded k extent per parity block in k_m2l
@@ -69,6 +72,10 @@ struct FmmPlan {
     float *Tm2l = nullptr;    // [49][2][NBmax(j)][KP(k)] parity blocks, k padded
     float *Tm2lc = nullptr;   // [49][even NE x NE | odd NO x NO] compact, j-major (low orders)
     int m2l_resident = 0;     // 1: k_m2l_res (all operators in shared memory)
+    int far_fused = 0;        // 1: P2M .. L2L in one cooperative launch (k_far)
+    int far_grid = 0;
+    size_t far_smem = 0;
+    struct FarSync *far_sync = nullptr;
     int m2l_tc = 0;           // 1: tensor-core M2L (gather + grouped tcgen05 GEMM)
     // tensor-core M2L: per parity block b, A'_b rows = every box of levels >= 2
     // grouped by parity class, each row [S_hi | S_hi | S_lo] over the class's
@@ -106,6 +113,7 @@ __global__ void k_l2p_p2p(const float *__restrict__ rho, const float *__restrict
                           const float *__restrict__ Vt, const float *__restrict__ Gn, float *__restrict__ phi,
                           FmmDev f, int far)
 {
+    pdl_begin();
     extern __shared__ float sm[];
     const int s = f.s, S3 = 3 * s, Z = f.Z;
     float *qn = sm;                         // [Z][3s][3s] neighbourhood charges
@@ -156,13 +164,36 @@ __global__ void k_l2p_p2p(const float *__restrict__ rho, const float *__restrict
 constexpr int BB = 8;         // leaf boxes per CTA along x in the leaf kernels
 constexpr int NSPLIT = 9;     // M2L offset groups (3 offsets each) -> partial locals
 
-// P2M: CTA = BB leaf boxes of one row; thread per coefficient; the boxes'
-// charges sit transposed in shared memory ([cell][box]) so one LDS.128 feeds 4 FMAs
+// P2M of one item = BB leaf boxes of one row: the boxes' charges are staged
+// transposed in shared memory ([cell][box]); thread per (box, coefficient),
+// each output summed over the cells in order.  Wt: [C][NR] weights (shared or
+// global memory).  q: C * BB floats of shared memory.
+__device__ __forceinline__ void p2m_item(const float *__restrict__ rho, const float *Wt, float *q,
+                                         float *__restrict__ Mleaf, const FmmDev &f, int by, int bx0)
+{
+    const int s = f.s;
+    for (int i = threadIdx.x; i < f.C * BB; i += blockDim.x) {
+        const int b = i % BB, c = i / BB;
+        const int x = (bx0 + b) * s + c % s, y = by * s + (c / s) % s, z = c / (s * s);
+        q[i] = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < BB * f.NR; e += blockDim.x) {
+        const int b = e / f.NR, k = e % f.NR;
+        float acc = 0.f;
+#pragma unroll 4
+        for (int c = 0; c < f.C; c++) acc = fmaf(Wt[(long long)c * f.NR + k], q[c * BB + b], acc);
+        if (bx0 + b < f.nb) Mleaf[((long long)by * f.nb + bx0 + b) * f.NR + k] = acc;
+    }
+    __syncthreads();
+}
+
+// P2M: CTA = one item (BB leaf boxes of one row)
 __global__ void __launch_bounds__(128) k_p2m_row(const float *__restrict__ rho, const float *__restrict__ Wg,
                                                  float *__restrict__ Mleaf, FmmDev f, int wsm)
 {
+    pdl_begin();
     extern __shared__ __align__(16) float q[];  // [C][BB], then W [C][NR] when wsm
-    const int by = blockIdx.y, bx0 = blockIdx.x * BB, s = f.s;
     const float *Wt = Wg;
     if (wsm) {
         float *Ws = q + f.C * BB;
@@ -171,34 +202,7 @@ __global__ void __launch_bounds__(128) k_p2m_row(const float *__restrict__ rho, 
             *reinterpret_cast<float4 *>(&Ws[i]) = __ldg(reinterpret_cast<const float4 *>(&Wg[i]));
         Wt = Ws;
     }
-    for (int i = threadIdx.x; i < f.C * BB; i += blockDim.x) {
-        const int b = i % BB, c = i / BB;
-        const int x = (bx0 + b) * s + c % s, y = by * s + (c / s) % s, z = c / (s * s);
-        q[i] = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < f.NR; k += blockDim.x) {
-        float acc[BB];
-#pragma unroll
-        for (int b = 0; b < BB; b++) acc[b] = 0.f;
-#pragma unroll 4
-        for (int c = 0; c < f.C; c++) {
-            const float w = Wt[(long long)c * f.NR + k];
-            const float4 qa = *reinterpret_cast<const float4 *>(&q[c * BB]);
-            const float4 qb = *reinterpret_cast<const float4 *>(&q[c * BB + 4]);
-            acc[0] = fmaf(w, qa.x, acc[0]);
-            acc[1] = fmaf(w, qa.y, acc[1]);
-            acc[2] = fmaf(w, qa.z, acc[2]);
-            acc[3] = fmaf(w, qa.w, acc[3]);
-            acc[4] = fmaf(w, qb.x, acc[4]);
-            acc[5] = fmaf(w, qb.y, acc[5]);
-            acc[6] = fmaf(w, qb.z, acc[6]);
-            acc[7] = fmaf(w, qb.w, acc[7]);
-        }
-#pragma unroll
-        for (int b = 0; b < BB; b++)
-            if (bx0 + b < f.nb) Mleaf[((long long)by * f.nb + bx0 + b) * f.NR + k] = acc[b];
-    }
+    p2m_item(rho, Wt, q, Mleaf, f, blockIdx.y, blockIdx.x * BB);
 }
 
 // M2M: CTA per parent box, thread per (child c, output coefficient k).  The
@@ -210,26 +214,22 @@ __device__ __forceinline__ int blk_base(int c, int NE, int NO, int blk)
     return c * (NE * NE + NO * NO) + (blk ? NE * NE : 0);
 }
 
-__global__ void k_m2m_c(float *__restrict__ Mall, const float *__restrict__ Tb, long long off_p, long long off_c,
-                        int np, FmmDev f)
+// one parent box of M2M with a group of 4 KT threads (t = thread in group):
+// thread (child c, coefficient k); Ts = the 4 child operators in shared
+// memory; Mc (4 NR) and red (4 KT) are the group's shared scratch
+__device__ __forceinline__ void m2m_item(float *__restrict__ Mall, const float *Ts, float *Mc, float *red,
+                                         long long off_p, long long off_c, int np, int box, const FmmDev &f, int t,
+                                         int KT, bool valid = true)
 {
-    extern __shared__ __align__(16) float smb[];
     const int NE = f.NE, NO = f.NR - f.NE;
-    const int tsz = 4 * (NE * NE + NO * NO);
-    const int KT = blockDim.x / 4;            // threads per child
-    float *Ts = smb;                          // [4][blocks]
-    float *Mc = smb + tsz;                    // [4][NR]
-    float *red = Mc + 4 * f.NR;               // [4][KT]
-    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
-    const int box = blockIdx.x, bx = box % np, by = box / np, nc = 2 * np;
-    for (int i = threadIdx.x; i < 4 * f.NR; i += blockDim.x) {
+    const int bx = box % np, by = box / np, nc = 2 * np;
+    for (int i = t; valid && i < 4 * f.NR; i += 4 * KT) {
         const int c = i / f.NR, j = i % f.NR;
         const int cx = 2 * bx + (c & 1), cy = 2 * by + (c >> 1);
         Mc[i] = Mall[(off_c + (long long)cy * nc + cx) * f.NR + j];
     }
     __syncthreads();
-    const int c = threadIdx.x / KT, k = threadIdx.x % KT;
+    const int c = t / KT, k = t % KT;
     float acc = 0.f;
     if (k < f.NR) {
         const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
@@ -240,8 +240,25 @@ __global__ void k_m2m_c(float *__restrict__ Mall, const float *__restrict__ Tb, 
     }
     red[c * KT + k] = acc;
     __syncthreads();
-    if (c == 0 && k < f.NR)
+    if (valid && c == 0 && k < f.NR)
         Mall[(off_p + box) * f.NR + k] = (red[k] + red[KT + k]) + (red[2 * KT + k] + red[3 * KT + k]);
+    __syncthreads();
+}
+
+__global__ void k_m2m_c(float *__restrict__ Mall, const float *__restrict__ Tb, long long off_p, long long off_c,
+                        int np, FmmDev f)
+{
+    pdl_begin();
+    extern __shared__ __align__(16) float smb[];
+    const int NE = f.NE, NO = f.NR - f.NE;
+    const int tsz = 4 * (NE * NE + NO * NO);
+    const int KT = blockDim.x / 4;            // threads per child
+    float *Ts = smb;                          // [4][blocks]
+    float *Mc = smb + tsz;                    // [4][NR]
+    float *red = Mc + 4 * f.NR;               // [4][KT]
+    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    m2m_item(Mall, Ts, Mc, red, off_p, off_c, np, blockIdx.x, f, threadIdx.x, KT);
 }
 
 // M2L, all levels >= 2 in one launch.  CTA = 32 targets of one (level, parity
@@ -259,6 +276,7 @@ __global__ void __launch_bounds__(32 * M2L_WARPS) k_m2l_split(const float *__res
                                                               const long long *__restrict__ lev_off, FmmDev f,
                                                               int KP0, int KP1, int NBmax, long long part_stride)
 {
+    pdl_begin();
     extern __shared__ __align__(16) float sm2[];
     const int4 it = items[blockIdx.x];
     const int lev = it.x, px = it.y & 1, py = it.y >> 1;
@@ -335,19 +353,16 @@ __global__ void __launch_bounds__(32 * M2L_WARPS) k_m2l_split(const float *__res
 // complete M2L local (one partial buffer).
 constexpr int RES_WARPS = 8;
 
-template <int NR_, int NE_>
-__global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restrict__ Mall, float *__restrict__ Lout,
-                                                            const float *__restrict__ Tc, const int4 *__restrict__ items,
-                                                            const long long *__restrict__ lev_off, FmmDev f)
+// one M2L item (32 targets of one level and parity class, all 27 offsets) on
+// RES_WARPS warps; Ts = all 49 operator slots in shared memory; red =
+// RES_WARPS * 32 * (NR + 1) floats of shared scratch (may alias Ts: it is
+// written only after the last operator read)
+template <int NR_, int NE_, bool NC>
+__device__ __forceinline__ void m2l_res_item(const float *__restrict__ Mall, float *__restrict__ Lout, const float *Ts,
+                                             float *red, const int4 it, const long long *__restrict__ lev_off)
 {
     constexpr int NO_ = NR_ - NE_;
     constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
-    extern __shared__ __align__(16) float sr[];
-    float *Ts = sr;                           // [49][OSZ], reused as [RES_WARPS][32][NR_ + 1]
-    float *red = sr;
-    for (int i = threadIdx.x * 4; i < 49 * OSZ; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tc[i]));
-    const int4 it = items[blockIdx.x];
     const int lev = it.x, px = it.y & 1, py = it.y >> 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n = 1 << lev, nh = n >> 1;
@@ -379,7 +394,7 @@ __global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restr
         const float2 *ms = reinterpret_cast<const float2 *>(Mall + (off + (long long)(ok ? sy : 0) * n + (ok ? sx : 0)) * NR_);
 #pragma unroll
         for (int v = 0; v < NR_ / 2; v++) {
-            const float2 u = ok ? __ldg(&ms[v]) : make_float2(0.f, 0.f);
+            const float2 u = ok ? (NC ? __ldg(&ms[v]) : ms[v]) : make_float2(0.f, 0.f);
             dst[2 * v] = u.x;
             dst[2 * v + 1] = u.y;
         }
@@ -415,7 +430,7 @@ __global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restr
 #pragma unroll
         for (int k = 0; k < NR_; k++) m[k] = mn[k];
     }
-    __syncthreads();  // operators no longer needed: the area becomes the reduction buffer
+    __syncthreads();  // (when red aliases Ts) operators no longer needed
     float *rw = red + (warp * 32 + lane) * (NR_ + 1);
 #pragma unroll
     for (int k = 0; k < NR_; k++) rw[k] = acc[k];
@@ -431,25 +446,75 @@ __global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restr
         const int ux = 2 * (tj % nh) + px, uy = 2 * (tj / nh) + py;
         Lout[(off + (long long)uy * n + ux) * NR_ + k] = v;
     }
+    __syncthreads();
+}
+
+template <int NR_, int NE_>
+__global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restrict__ Mall, float *__restrict__ Lout,
+                                                            const float *__restrict__ Tc, const int4 *__restrict__ items,
+                                                            const long long *__restrict__ lev_off, FmmDev f)
+{
+    pdl_begin();
+    constexpr int NO_ = NR_ - NE_;
+    constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
+    extern __shared__ __align__(16) float sr[];
+    for (int i = threadIdx.x * 4; i < 49 * OSZ; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&sr[i]) = __ldg(reinterpret_cast<const float4 *>(&Tc[i]));
+    (void)f;
+    m2l_res_item<NR_, NE_, true>(Mall, Lout, sr, sr, items[blockIdx.x], lev_off);
+}
+
+// one parent box of the downward pass with a group of 4 KT threads: child
+// locals = L2L of the parent's final local + the M2L partials; Ts = the 4
+// operators in shared memory; Lp = NR floats of the group's shared scratch
+__device__ __forceinline__ void l2l_item(float *__restrict__ Lfin, const float *__restrict__ Lpart, const float *Ts,
+                                         float *Lp, long long off_p, long long off_c, int nc, int np, int pb,
+                                         long long part_stride, int nsplit, const FmmDev &f, int t, int KT,
+                                         bool valid = true)
+{
+    const int NE = f.NE, NO = f.NR - f.NE;
+    for (int i = t; valid && i < f.NR; i += 4 * KT) Lp[i] = Lfin[(off_p + pb) * (long long)f.NR + i];
+    __syncthreads();
+    const int c = t / KT, k = t % KT;
+    if (valid && k < f.NR) {
+        const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+        const float *T = Ts + blk_base(c, NE, NO, blk);
+        const float *lp = Lp + boff;
+        float acc = 0.f;
+#pragma unroll 8
+        for (int j = 0; j < NB; j++) acc = fmaf(T[j * NB + kk], lp[j], acc);
+        const int cx = 2 * (pb % np) + (c & 1), cy = 2 * (pb / np) + (c >> 1);
+        const long long b = off_c + (long long)cy * nc + cx;
+        float v = acc;
+        for (int g = 0; g < nsplit; g++) v += Lpart[g * part_stride + b * f.NR + k];
+        Lfin[b * f.NR + k] = v;
+    }
+    __syncthreads();
+}
+
+// level 2 has no far-field parent: its locals are the partial sums alone
+__device__ __forceinline__ void l2l_top_box(float *__restrict__ Lfin, const float *__restrict__ Lpart, long long b,
+                                            long long part_stride, int nsplit, const FmmDev &f, int t, int nt)
+{
+    for (int k = t; k < f.NR; k += nt) {
+        float v = 0.f;
+        for (int g = 0; g < nsplit; g++) v += Lpart[g * part_stride + b * f.NR + k];
+        Lfin[b * f.NR + k] = v;
+    }
 }
 
 // Downward pass of one level: L(child) = sum of the NSPLIT M2L partials of the
 // child (fixed order) + L2L of the final parent local.  CTA per parent box,
 // thread per (child c, coefficient k); operator blocks and the parent local
-// staged in shared memory.  np == 0 is level 2, which has no far-field
-// parent: its locals are the partial sums alone (CTA per box).
+// staged in shared memory.  np == 0 is level 2 (CTA per box).
 __global__ void k_l2l_c(float *__restrict__ Lfin, const float *__restrict__ Lpart, const float *__restrict__ Tb,
                         long long off_p, long long off_c, int nc, int np, long long part_stride, int nsplit, FmmDev f)
 {
+    pdl_begin();
     extern __shared__ __align__(16) float smb[];
     const int NE = f.NE, NO = f.NR - f.NE;
     if (np == 0) {
-        const long long b = off_c + blockIdx.x;
-        for (int k = threadIdx.x; k < f.NR; k += blockDim.x) {
-            float v = 0.f;
-            for (int g = 0; g < nsplit; g++) v += Lpart[g * part_stride + b * f.NR + k];
-            Lfin[b * f.NR + k] = v;
-        }
+        l2l_top_box(Lfin, Lpart, off_c + blockIdx.x, part_stride, nsplit, f, threadIdx.x, blockDim.x);
         return;
     }
     const int tsz = 4 * (NE * NE + NO * NO);
@@ -458,22 +523,147 @@ __global__ void k_l2l_c(float *__restrict__ Lfin, const float *__restrict__ Lpar
     float *Lp = smb + tsz;    // [NR]
     for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
         *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
-    const int pb = blockIdx.x;
-    for (int i = threadIdx.x; i < f.NR; i += blockDim.x) Lp[i] = Lfin[(off_p + pb) * (long long)f.NR + i];
+    l2l_item(Lfin, Lpart, Ts, Lp, off_p, off_c, nc, np, blockIdx.x, part_stride, nsplit, f, threadIdx.x, KT);
+}
+
+// Fused far field (P <= 4, solver far_mode 1): ONE cooperative launch (one
+// CTA per SM, all co-resident) runs P2M, the M2M levels L-1 .. 2, the
+// resident M2L of every level and the L2L levels 2 .. L-1, with a grid
+// barrier between dependent phases, instead of 2 L - 1 short launches.  At
+// 256 x 256 x 3 it measured slower than the per-stage launches (9 barriers
+// and thinly filled upper-level phases cost more than the launches they
+// save, and its shared memory keeps the concurrent near field off the SMs),
+// so it is an option, not the default.  Each CTA keeps the M2M, L2L and
+// all 49 M2L operator slots in shared memory; the M2L table streams in with
+// cp.async while the upward pass runs.  Every item runs the same code (and
+// summation order) as the per-stage kernels, so both paths give identical
+// bits.  Data written inside the launch is read with ordinary loads after the
+// barrier's gpu-scope acquire, never through the non-coherent (ld.global.nc)
+// path.
+}  // namespace
+
+struct FarSync {
+    unsigned count;  // CTAs arrived at the current barrier (returns to 0)
+    unsigned gen;    // barrier generation
+    int err;         // 1: a barrier wait timed out
+    int pad;
+};
+
+namespace {
+
+constexpr long long BARRIER_CYCLES = 2000000000LL;  // ~1 s
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// all CTAs of the (cooperative) grid; bounded: a wait longer than ~1 s sets
+// sy->err and returns
+__device__ void grid_barrier(FarSync *sy)
+{
     __syncthreads();
-    const int c = threadIdx.x / KT, k = threadIdx.x % KT;
-    if (k >= f.NR) return;
-    const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
-    const float *T = Ts + blk_base(c, NE, NO, blk);
-    const float *lp = Lp + boff;
-    float acc = 0.f;
-#pragma unroll 8
-    for (int j = 0; j < NB; j++) acc = fmaf(T[j * NB + kk], lp[j], acc);
-    const int cx = 2 * (pb % np) + (c & 1), cy = 2 * (pb / np) + (c >> 1);
-    const long long b = off_c + (long long)cy * nc + cx;
-    float v = acc;
-    for (int g = 0; g < nsplit; g++) v += Lpart[g * part_stride + b * f.NR + k];
-    Lfin[b * f.NR + k] = v;
+    if (threadIdx.x == 0) {
+        const unsigned g = ld_acquire_u32(&sy->gen);
+        __threadfence();
+        if (atomicAdd(&sy->count, 1u) == gridDim.x - 1) {
+            atomicExch(&sy->count, 0u);
+            __threadfence();
+            atomicAdd(&sy->gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (ld_acquire_u32(&sy->gen) == g) {
+                if (clock64() - t0 > BARRIER_CYCLES) {
+                    atomicExch(&sy->err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+template <int NR_>
+__host__ __device__ constexpr int far_kt() { return ((NR_ + 31) / 32) * 32; }
+
+template <int NR_, int NE_>
+constexpr int far_scratch(int C)
+{
+    constexpr int KT = far_kt<NR_>();
+    constexpr int G = (32 * RES_WARPS) / (4 * KT);
+    const int a = C * BB, b = RES_WARPS * 32 * (NR_ + 1), c = G * (4 * NR_ + 4 * KT + NR_);
+    return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
+
+template <int NR_, int NE_>
+__global__ void __launch_bounds__(32 * RES_WARPS) k_far(const float *__restrict__ rho, const float *__restrict__ Wg,
+                                                        float *__restrict__ Mall, float *__restrict__ Lpart,
+                                                        float *__restrict__ Lall, const float *__restrict__ Tm2m,
+                                                        const float *__restrict__ Tm2lc,
+                                                        const float *__restrict__ Tl2l, const int4 *__restrict__ items,
+                                                        int nitems, const long long *__restrict__ lev_off, FmmDev f,
+                                                        int nbx, int nby, int lend, FarSync *sy)
+{
+    constexpr int NO_ = NR_ - NE_;
+    constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
+    constexpr int KT = far_kt<NR_>();
+    constexpr int G = (32 * RES_WARPS) / (4 * KT);  // parent boxes per pass in M2M / L2L
+    static_assert((49 * OSZ) % 4 == 0 && G >= 1, "operator table must be whole float4s");
+    extern __shared__ __align__(16) float sf[];
+    float *Tl = sf;                 // [49][OSZ] M2L
+    float *Tu = Tl + 49 * OSZ;      // [4 OSZ]  M2M
+    float *Td = Tu + 4 * OSZ;       // [4 OSZ]  L2L
+    float *scr = Td + 4 * OSZ;      // P2M charges | M2L reduction | per-group M2M/L2L scratch
+    const int tid = threadIdx.x;
+    for (int i = tid * 4; i < 49 * OSZ; i += blockDim.x * 4)
+        umma::cp_async16(umma::smem_u32(Tl + i), Tm2lc + i, true);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    for (int i = tid * 4; i < 4 * OSZ; i += blockDim.x * 4) {
+        *reinterpret_cast<float4 *>(&Tu[i]) = __ldg(reinterpret_cast<const float4 *>(&Tm2m[i]));
+        *reinterpret_cast<float4 *>(&Td[i]) = __ldg(reinterpret_cast<const float4 *>(&Tl2l[i]));
+    }
+    __syncthreads();
+    const int grp = tid / (4 * KT), t = tid % (4 * KT);
+    float *Mc = scr + grp * (4 * NR_ + 4 * KT + NR_);  // group scratch: [4 NR] children, [4 KT] partials
+    float *red = Mc + 4 * NR_;
+    float *Lp = red + 4 * KT;                           // [NR] parent local (L2L)
+
+    // P2M: items of BB leaf boxes along a row
+    const int rowitems = (nbx + BB - 1) / BB;
+    for (int it = blockIdx.x; it < rowitems * nby; it += gridDim.x)
+        p2m_item(rho, Wg, scr, Mall + lev_off[f.L] * NR_, f, it / rowitems, (it % rowitems) * BB);
+    grid_barrier(sy);
+    // M2M: level L-1 .. 2
+    for (int l = f.L - 1; l >= 2; l--) {
+        const int np = 1 << l;
+        for (int base = blockIdx.x * G; base < np * np; base += gridDim.x * G) {
+            const int box = base + grp;
+            m2m_item(Mall, Tu, Mc, red, lev_off[l], lev_off[l + 1], np, box, f, t, KT, grp < G && box < np * np);
+        }
+        grid_barrier(sy);
+    }
+    // M2L, every level
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) m2l_res_item<NR_, NE_, false>(Mall, Lpart, Tl, scr, items[it], lev_off);
+    // L2L: level 2 from its partials, then 3 .. lend
+    if (lend >= 2) {
+        grid_barrier(sy);
+        for (int b = blockIdx.x; b < 16; b += gridDim.x) l2l_top_box(Lall, Lpart, lev_off[2] + b, 0, 1, f, tid, blockDim.x);
+        for (int l = 3; l <= lend; l++) {
+            grid_barrier(sy);
+            const int nc = 1 << l, np = nc / 2;
+            for (int base = blockIdx.x * G; base < np * np; base += gridDim.x * G) {
+                const int pb = base + grp;
+                l2l_item(Lall, Lpart, Td, Lp, lev_off[l - 1], lev_off[l], nc, np, pb, 0, 1, f, t, KT,
+                         grp < G && pb < np * np);
+            }
+        }
+    }
 }
 
 // Leaf kernels.  The near field (P2P) needs only the charges, so it runs on a
@@ -489,6 +679,7 @@ template <int S, int BB>
 __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, const float *__restrict__ Gn,
                                               float *__restrict__ out, FmmDev f)
 {
+    pdl_begin();
     extern __shared__ __align__(16) float sl[];
     const int Z = f.Z;
     constexpr int W = (BB + 2) * S;        // charges per staged row
@@ -559,6 +750,7 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
                                               const float *__restrict__ Vt, float *__restrict__ phi, FmmDev f,
                                               long long part_stride, int nsplit)
 {
+    pdl_begin();
     extern __shared__ __align__(16) float sl[];
     const int Z = f.Z;
     const int NE = f.NE, NO = f.NR - f.NE;
@@ -762,7 +954,7 @@ int leaf_set_smem(const FmmDev &f)
 int p2p_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float *Gn, float *out, cudaStream_t st)
 {
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
-#define X(S_, B_) if (f.s == S_) { k_p2p<S_, B_><<<grid, leaf_threads(f), p2p_smem(f), st>>>(rho, Gn, out, f); return MMS_OK; }
+#define X(S_, B_) if (f.s == S_) { MMS_CUDA_TRY(launch_k(k_p2p<S_, B_>, grid, dim3(leaf_threads(f)), p2p_smem(f), st, rho, Gn, out, f)); return MMS_OK; }
     MMS_LEAF_CASES(X)
 #undef X
     mms_set_error("no leaf kernel for side %d", f.s);
@@ -773,7 +965,7 @@ int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float
                const float *Tl2l, const float *Vt, float *phi, long long part_stride, int nsplit, cudaStream_t st)
 {
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
-#define X(S_, B_) if (f.s == S_) { k_l2p<S_, B_><<<grid, leaf_threads(f), l2p_smem(f), st>>>(near, Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit); return MMS_OK; }
+#define X(S_, B_) if (f.s == S_) { MMS_CUDA_TRY(launch_k(k_l2p<S_, B_>, grid, dim3(leaf_threads(f)), l2p_smem(f), st, near, Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit)); return MMS_OK; }
     MMS_LEAF_CASES(X)
 #undef X
     mms_set_error("no leaf kernel for side %d", f.s);
@@ -815,7 +1007,7 @@ int m2l_res_launch(const FmmDev &f, int nitems, const float *Mall, float *Lout, 
                    const long long *lev, cudaStream_t st)
 {
     const size_t sm = m2l_res_smem(f.NR, f.NE);
-#define X(a, c) if (f.NR == a && f.NE == c) { k_m2l_res<a, c><<<nitems, 32 * RES_WARPS, sm, st>>>(Mall, Lout, Tc, items, lev, f); return MMS_OK; }
+#define X(a, c) if (f.NR == a && f.NE == c) { MMS_CUDA_TRY(launch_k(k_m2l_res<a, c>, dim3(nitems), dim3(32 * RES_WARPS), sm, st, Mall, Lout, Tc, items, lev, f)); return MMS_OK; }
     MMS_M2L_RES_CASES(X)
 #undef X
     mms_set_error("no resident M2L kernel for NR=%d", f.NR);
@@ -824,6 +1016,7 @@ int m2l_res_launch(const FmmDev &f, int nitems, const float *Mall, float *Lout, 
 }  // namespace
 
 int fmm_default_leaf(int P, int X, int Y);
+int far_prepare(mms_ctx *ctx, FmmPlan *pl);
 
 int fmm_plan_create(mms_ctx *ctx)
 {
@@ -1117,6 +1310,8 @@ int fmm_plan_create(mms_ctx *ctx)
     if (m2ls_smem > 48 * 1024)
         MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2l_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)m2ls_smem));
     if (pl->m2l_resident) MMS_TRY(m2l_res_prepare(NR, f.NE));
+    if (pl->m2l_resident && NR <= 30 && leaf_threads(f) > 0 && f.L >= 2 && ctx->s.far_mode == 1)
+        MMS_TRY(far_prepare(ctx, pl));
     {
         const size_t pm = (size_t)f.C * (BB + f.NR) * sizeof(float);
         if (pm > 48 * 1024 && pm <= 160 * 1024)
@@ -1186,7 +1381,7 @@ void fmm_plan_destroy(mms_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Tm2lc, pl->Gn, pl->Mall, pl->Lall, pl->Lpart,
                  pl->m2l_items, pl->lev_dev, pl->near, pl->tcA[0], pl->tcA[1], pl->tcB, pl->tc_rowmap,
-                 pl->tc_rowinfo, pl->tc_groups};
+                 pl->tc_rowinfo, pl->tc_groups, pl->far_sync};
     for (void *p : b)
         if (p) cudaFree(p);
     if (pl->side) cudaStreamSynchronize(pl->side);
@@ -1234,16 +1429,18 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     case 0: {
         const long long leaf_off = pl->lev_off[f.L];
         const int wsm = (f.C * f.NR) % 4 == 0 && (size_t)f.C * (BB + f.NR) * sizeof(float) <= 160 * 1024;
-        k_p2m_row<<<dim3(div_up(nbx, BB), nby), 128, (size_t)f.C * (BB + (wsm ? f.NR : 0)) * sizeof(float),
-                    ctx->stream>>>(rho, pl->Wt, pl->Mall + leaf_off * f.NR, f, wsm);
+        MMS_CUDA_TRY(launch_k(k_p2m_row, dim3(div_up(nbx, BB), nby), dim3(128),
+                              (size_t)f.C * (BB + (wsm ? f.NR : 0)) * sizeof(float), ctx->stream, rho,
+                              (const float *)pl->Wt, pl->Mall + leaf_off * f.NR, f, wsm));
         MMS_LAUNCH_CHECK(ctx);
         break;
     }
     case 1:
         for (int l = f.L - 1; l >= 2; l--) {
             const int np = 1 << l;
-            k_m2m_c<<<np * np, 4 * KT, (tsz + 4 * (size_t)f.NR + 4 * (size_t)KT) * sizeof(float), ctx->stream>>>(
-                pl->Mall, pl->Tm2m, pl->lev_off[l], pl->lev_off[l + 1], np, f);
+            MMS_CUDA_TRY(launch_k(k_m2m_c, dim3(np * np), dim3(4 * KT),
+                                  (tsz + 4 * (size_t)f.NR + 4 * (size_t)KT) * sizeof(float), ctx->stream, pl->Mall,
+                                  (const float *)pl->Tm2m, pl->lev_off[l], pl->lev_off[l + 1], np, f));
             MMS_LAUNCH_CHECK(ctx);
         }
         break;
@@ -1265,9 +1462,10 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
             const int NBmax = std::max(f.NE, f.NR - f.NE);
             const int KPmax = std::max(pl->KPb[0], pl->KPb[1]);
             const size_t sm = ((size_t)NBmax * KPmax + 32 * (size_t)(NBmax | 1)) * sizeof(float);
-            k_m2l_split<<<dim3(pl->n_m2l_items, 2, NSPLIT), 32 * M2L_WARPS, sm, ctx->stream>>>(
-                pl->Mall, pl->Lpart, pl->Tm2l, pl->m2l_items, pl->lev_dev, f, pl->KPb[0], pl->KPb[1], NBmax,
-                part_stride);
+            MMS_CUDA_TRY(launch_k(k_m2l_split, dim3(pl->n_m2l_items, 2, NSPLIT), dim3(32 * M2L_WARPS), sm,
+                                  ctx->stream, (const float *)pl->Mall, pl->Lpart, (const float *)pl->Tm2l,
+                                  (const int4 *)pl->m2l_items, (const long long *)pl->lev_dev, f, pl->KPb[0],
+                                  pl->KPb[1], NBmax, part_stride));
         }
         MMS_LAUNCH_CHECK(ctx);
         break;
@@ -1278,14 +1476,16 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         // generic leaf kernel)
         const int lend = leaf_threads(f) > 0 ? f.L - 1 : f.L;
         if (lend >= 2) {
-            k_l2l_c<<<16, thr, 0, ctx->stream>>>(pl->Lall, pl->Lpart, pl->Tl2l, 0, pl->lev_off[2], 4, 0,
-                                                 part_stride, nsplit, f);
+            MMS_CUDA_TRY(launch_k(k_l2l_c, dim3(16), dim3(thr), 0, ctx->stream, pl->Lall,
+                                  (const float *)pl->Lpart, (const float *)pl->Tl2l, 0LL, pl->lev_off[2], 4, 0,
+                                  part_stride, nsplit, f));
             MMS_LAUNCH_CHECK(ctx);
         }
         for (int l = 3; l <= lend; l++) {
             const int nc = 1 << l, np = nc / 2;
-            k_l2l_c<<<np * np, 4 * KT, (tsz + (size_t)f.NR) * sizeof(float), ctx->stream>>>(
-                pl->Lall, pl->Lpart, pl->Tl2l, pl->lev_off[l - 1], pl->lev_off[l], nc, np, part_stride, nsplit, f);
+            MMS_CUDA_TRY(launch_k(k_l2l_c, dim3(np * np), dim3(4 * KT), (tsz + (size_t)f.NR) * sizeof(float),
+                                  ctx->stream, pl->Lall, (const float *)pl->Lpart, (const float *)pl->Tl2l,
+                                  pl->lev_off[l - 1], pl->lev_off[l], nc, np, part_stride, nsplit, f));
             MMS_LAUNCH_CHECK(ctx);
         }
         break;
@@ -1315,6 +1515,82 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     return MMS_OK;
 }
 
+#define MMS_FAR_CASES(X) X(6, 4) X(12, 8) X(20, 12) X(30, 18)
+
+// sizes and enables the fused far-field kernel; leaves it off (per-stage
+// kernels) when the device cannot co-schedule one CTA per SM
+int far_prepare(mms_ctx *ctx, FmmPlan *pl)
+{
+    const FmmDev &f = pl->d;
+    int coop = 0, sms = 0;
+    MMS_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+    MMS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    if (!coop) return MMS_OK;
+    const int NO = f.NR - f.NE, OSZ = f.NE * f.NE + NO * NO;
+    int scratch = 0, occ = 0;
+#define X(a, c)                                                                                      \
+    if (f.NR == a && f.NE == c) {                                                                    \
+        scratch = far_scratch<a, c>(f.C);                                                            \
+        pl->far_smem = (size_t)(57 * OSZ + scratch) * sizeof(float);                                 \
+        if (pl->far_smem > 227 * 1024) return MMS_OK;                                                \
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_far<a, c>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                          (int)pl->far_smem));                                      \
+        MMS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_far<a, c>, 32 * RES_WARPS, \
+                                                                   pl->far_smem));                   \
+    }
+    MMS_FAR_CASES(X)
+#undef X
+    if (occ < 1) return MMS_OK;
+    if (cudaMalloc((void **)&pl->far_sync, sizeof(FarSync)) != cudaSuccess) {
+        mms_set_error("FMM plan: device allocation failed");
+        return MMS_ERR_NOMEM;
+    }
+    MMS_CUDA_TRY(cudaMemset(pl->far_sync, 0, sizeof(FarSync)));
+    pl->far_grid = sms;  // one CTA per SM: co-resident with room to spare
+    pl->far_fused = 1;
+    return MMS_OK;
+}
+
+int far_launch(mms_ctx *ctx, const float *rho)
+{
+    FmmPlan *pl = ctx->fmm;
+    const FmmDev &f = pl->d;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    const int lend = f.L - 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(pl->far_grid);
+    cfg.blockDim = dim3(32 * RES_WARPS);
+    cfg.dynamicSmemBytes = pl->far_smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+#define X(a, c)                                                                                                   \
+    if (f.NR == a && f.NE == c) {                                                                                 \
+        MMS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_far<a, c>, rho, (const float *)pl->Wt, pl->Mall, pl->Lpart,        \
+                                        pl->Lall, (const float *)pl->Tm2m, (const float *)pl->Tm2lc,                \
+                                        (const float *)pl->Tl2l, (const int4 *)pl->m2l_items, pl->n_m2l_items,      \
+                                        (const long long *)pl->lev_dev, f, nbx, nby, lend, pl->far_sync));         \
+        MMS_LAUNCH_CHECK(ctx);                                                                                    \
+        return MMS_OK;                                                                                            \
+    }
+    MMS_FAR_CASES(X)
+#undef X
+    mms_set_error("no fused far-field kernel for NR=%d", f.NR);
+    return MMS_ERR_ARG;
+}
+
+// 1 when a barrier of the fused far-field kernel timed out since the plan was made
+int fmm_far_error(mms_ctx *ctx)
+{
+    if (!ctx->fmm || !ctx->fmm->far_sync) return 0;
+    FarSync h{};
+    if (cudaMemcpy(&h, ctx->fmm->far_sync, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+    return h.err != 0;
+}
+
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
 {
     FmmPlan *pl = ctx->fmm;
@@ -1334,7 +1610,10 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
     MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, pl->side));
     MMS_LAUNCH_CHECK(ctx);
     MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
-    for (int st = 0; st < 4; st++) MMS_TRY(launch_fmm_stage(ctx, st, rho, phi));
+    if (pl->far_fused)
+        MMS_TRY(far_launch(ctx, rho));
+    else
+        for (int st = 0; st < 4; st++) MMS_TRY(launch_fmm_stage(ctx, st, rho, phi));
     MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
     return l2p_launch_far(ctx, rho, phi);
 }

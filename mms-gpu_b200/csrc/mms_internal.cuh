@@ -153,6 +153,7 @@ void sno_set_fast(mms_sno *n, bool fast);
 int rel_l2_dev(mms_ctx *ctx, const float *a, const float *b, long long n, double *out);
 void fmm_plan_destroy(mms_ctx *ctx);
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi);
+int fmm_far_error(mms_ctx *ctx);  // 1: a fused far-field barrier timed out
 size_t fmm_plan_bytes(const mms_ctx *ctx);
 
 // tcgen05 BF16 GEMM (gemm.cu): C (+)= A B^T, A M x K, B N x K, K-major
@@ -162,6 +163,40 @@ int umma_check_error();
 
 // potential with the context's solver
 int launch_potential(mms_ctx *ctx, const float *rho, float *phi);
+
+// ---------------------------------------------------------------------------
+// programmatic dependent launch: a kernel launched by launch_k may be scheduled
+// while its stream predecessor is still running.  Every kernel launched this
+// way starts with pdl_begin(): it waits for the predecessor grid's completion
+// (and memory) before touching any input, then lets its own successor be
+// scheduled.  The overlap hides launch and ramp-up latency between the many
+// short kernels of a field evaluation.  MMS_PDL=0 in the environment turns the
+// attribute off (plain stream order).
+bool pdl_enabled();
+
+__device__ __forceinline__ void pdl_begin()
+{
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+#ifdef MMS_PDL_EARLY_TRIGGER
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+#endif
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 
 // device allocation tracked in ctx->dev_bytes
 template <class T>

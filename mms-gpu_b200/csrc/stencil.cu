@@ -144,6 +144,7 @@ __global__ void k_hfield_aos(const float *__restrict__ M, const float *__restric
 
 __global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho, GridK g)
 {
+    pdl_begin();
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= g.N) return;
     int x, y, z;
@@ -171,6 +172,7 @@ __global__ void __launch_bounds__(TPB) k_rk4_stage(const float *__restrict__ phi
                                                    const double *__restrict__ tstate, const double *__restrict__ htab,
                                                    double *__restrict__ stats, GridK g, PhysK p, int stage)
 {
+    pdl_begin();
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= g.N) return;
     const long long N = g.N;
@@ -234,6 +236,7 @@ __global__ void __launch_bounds__(TPB) k_rk4_stage(const float *__restrict__ phi
 
 __global__ void k_advance_time(double *tstate)
 {
+    pdl_begin();
     // t_k1: time at which the next step's k1 field is taken.  The reference
     // evaluates the post-step field at the OLD t (ode_functions.cpp:267).
     tstate[TIME_TK1] = tstate[TIME_T];
@@ -384,7 +387,7 @@ int launch_divergence_aos(mms_ctx *ctx, const float *M, float *rho)
 
 int launch_divergence_soa(mms_ctx *ctx, const double *M, float *rho)
 {
-    k_div_soa<<<div_up(ctx->N, TPB), TPB, 0, ctx->stream>>>(M, rho, ctx->gk());
+    MMS_CUDA_TRY(launch_k(k_div_soa, dim3(div_up(ctx->N, TPB)), dim3(TPB), 0, ctx->stream, M, rho, ctx->gk()));
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
@@ -413,16 +416,17 @@ int launch_hfield_aos(mms_ctx *ctx, const float *M, const float *phi, double t, 
 
 int launch_rk4_stage(mms_ctx *ctx, int stage, const double *Mst, double *Mnext)
 {
-    k_rk4_stage<<<div_up(ctx->N, TPB), TPB, 0, ctx->stream>>>(ctx->phi, Mst, ctx->M, ctx->K, Mnext, ctx->mat,
-                                                             ctx->tstate, ctx->hext, ctx->stats, ctx->gk(),
-                                                             ctx->pk(), stage);
+    MMS_CUDA_TRY(launch_k(k_rk4_stage, dim3(div_up(ctx->N, TPB)), dim3(TPB), 0, ctx->stream,
+                          (const float *)ctx->phi, Mst, ctx->M, ctx->K, Mnext, (const uint8_t *)ctx->mat,
+                          (const double *)ctx->tstate, (const double *)ctx->hext, ctx->stats, ctx->gk(),
+                          ctx->pk(), stage));
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
 
 int launch_advance_time(mms_ctx *ctx)
 {
-    k_advance_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate);
+    MMS_CUDA_TRY(launch_k(k_advance_time, dim3(1), dim3(1), 0, ctx->stream, ctx->tstate));
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }

@@ -77,9 +77,11 @@ namespace {
 struct Key {
     int X, Y, Z;
     long long dxq, dyq, dzq, tolq;
+    int steps;  // 1: timed on RK4 steps of a state
     bool operator<(const Key &o) const
     {
-        return std::tie(X, Y, Z, dxq, dyq, dzq, tolq) < std::tie(o.X, o.Y, o.Z, o.dxq, o.dyq, o.dzq, o.tolq);
+        return std::tie(X, Y, Z, dxq, dyq, dzq, tolq, steps) <
+               std::tie(o.X, o.Y, o.Z, o.dxq, o.dyq, o.dzq, o.tolq, o.steps);
     }
 };
 
@@ -93,8 +95,14 @@ std::map<Key, Result> g_cache;
 
 }  // namespace
 
-extern "C" int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, const float *rho_dev,
-                                double max_rel_err, int reps, mms_solver *best, double *best_ms, double *best_err)
+namespace {
+
+// shared search: error on rho_dev against the exact sum; time = mean potential
+// evaluation (material == NULL) or mean graph-captured RK4 step of the state
+// (material, M) with step dt
+int autotune(const mms_grid *grid, const mms_params *params, const float *rho_dev, const uint8_t *material,
+             const double *M, double dt, double max_rel_err, int reps, mms_solver *best, double *best_ms,
+             double *best_err)
 {
     if (!grid || !params || !rho_dev || !best || !(max_rel_err > 0)) {
         mms_set_error("mms_autotune_fmm: bad argument");
@@ -102,7 +110,7 @@ extern "C" int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, 
     }
     if (reps < 1) reps = 5;
     const Key key{grid->xdim, grid->ydim, grid->zdim, llround(grid->dx * 1e15), llround(grid->dy * 1e15),
-                  llround(grid->dz * 1e15), llround(log10(max_rel_err) * 100)};
+                  llround(grid->dz * 1e15), llround(log10(max_rel_err) * 100), material ? 1 : 0};
     {
         std::lock_guard<std::mutex> lk(g_mu);
         auto it = g_cache.find(key);
@@ -143,6 +151,7 @@ extern "C" int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, 
         for (int P : orders)
             for (int s : leaves)
                 for (int m : modes) {
+                    if (st != MMS_OK) break;
                     mms_solver c;
                     memset(&c, 0, sizeof c);
                     c.kind = MMS_SOLVER_FMM;
@@ -166,9 +175,18 @@ extern "C" int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, 
                     }
                     const double err = b2 > 0 ? sqrt(d2 / b2) : 0.0;
                     if (!(err <= max_rel_err)) continue;
-                    cudaEventRecord(e0, ctx->stream);
-                    for (int r = 0; r < reps; r++) launch_potential(ctx, rho_dev, phi);
-                    cudaEventRecord(e1, ctx->stream);
+                    if (material) {
+                        // the same start state for every candidate; warm-up captures the graph
+                        if ((st = mms_state_set(ctx, material, M, 0.0)) || (st = mms_run_fixed(ctx, dt, 2, 1)))
+                            break;
+                        cudaEventRecord(e0, ctx->stream);
+                        if ((st = mms_run_fixed(ctx, dt, reps, 1))) break;
+                        cudaEventRecord(e1, ctx->stream);
+                    } else {
+                        cudaEventRecord(e0, ctx->stream);
+                        for (int r = 0; r < reps; r++) launch_potential(ctx, rho_dev, phi);
+                        cudaEventRecord(e1, ctx->stream);
+                    }
                     cudaEventSynchronize(e1);
                     float ms = 0.f;
                     cudaEventElapsedTime(&ms, e0, e1);
@@ -200,4 +218,23 @@ extern "C" int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, 
     if (best_ms) *best_ms = bestr.ms;
     if (best_err) *best_err = bestr.err;
     return MMS_OK;
+}
+
+}  // namespace
+
+extern "C" int mms_autotune_fmm(const mms_grid *grid, const mms_params *params, const float *rho_dev,
+                                double max_rel_err, int reps, mms_solver *best, double *best_ms, double *best_err)
+{
+    return autotune(grid, params, rho_dev, nullptr, nullptr, 0.0, max_rel_err, reps, best, best_ms, best_err);
+}
+
+extern "C" int mms_autotune_fmm_steps(const mms_grid *grid, const mms_params *params, const uint8_t *material,
+                                      const double *M, double dt, const float *rho_dev, double max_rel_err,
+                                      int reps, mms_solver *best, double *best_ms, double *best_err)
+{
+    if (!material || !M || !(dt > 0)) {
+        mms_set_error("mms_autotune_fmm_steps: bad argument");
+        return MMS_ERR_ARG;
+    }
+    return autotune(grid, params, rho_dev, material, M, dt, max_rel_err, reps, best, best_ms, best_err);
 }

@@ -58,7 +58,7 @@ class Params(ctypes.Structure):
 
 class Solver(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("fmm_order", ctypes.c_int), ("fmm_leaf", ctypes.c_int),
-                ("m2l_mode", ctypes.c_int), ("reserved", ctypes.c_int * 4)]
+                ("m2l_mode", ctypes.c_int), ("far_mode", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 class Controller(ctypes.Structure):
@@ -107,6 +107,8 @@ SIGNATURES = {
     "mms_diag_fma_tflops": (_I, [_I, ctypes.POINTER(_D)]),
     "mms_autotune_fmm": (_I, [ctypes.POINTER(Grid), ctypes.POINTER(Params), _VP, _D, _I, ctypes.POINTER(Solver),
                               ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "mms_autotune_fmm_steps": (_I, [ctypes.POINTER(Grid), ctypes.POINTER(Params), _VP, _VP, _D, _VP, _D, _I,
+                                    ctypes.POINTER(Solver), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "mms_diag_gemm_bf16": (_I, [_VP, _I, _VP, _I, _VP, _I, _I, _I, _I, _I, _I, _VP]),
     "mms_potential_direct_noalloc": (_I, [_VP, _VP, _I, _I, _I, _D, _D, _D, _VP]),
     "mms_ens_create": (_I, [_VP, _I, _D, _D, _D, ctypes.POINTER(Params), _VP, ctypes.POINTER(_VP)]),
@@ -208,6 +210,21 @@ def autotune_fmm(grid, params, rho_dev, max_rel_err=5e-4, reps=5):
     return best, ms.value, err.value
 
 
+def autotune_fmm_steps(grid, params, material, M, dt, rho_dev, max_rel_err=5e-4, reps=20):
+    """as autotune_fmm, but each candidate is timed on graph-captured RK4 steps
+    of size dt from the host state (material, M); returns (Solver, ms per step,
+    rel-L2 error)"""
+    p = params[0] if isinstance(params, tuple) else params
+    mat = np.ascontiguousarray(material, np.uint8)
+    Mh = np.ascontiguousarray(M, np.float64)
+    best = Solver()
+    ms, err = ctypes.c_double(), ctypes.c_double()
+    _check(load().mms_autotune_fmm_steps(ctypes.byref(grid), ctypes.byref(p), _ptr(mat), _ptr(Mh), dt,
+                                         _ptr(rho_dev), max_rel_err, reps, ctypes.byref(best), ctypes.byref(ms),
+                                         ctypes.byref(err)))
+    return best, ms.value, err.value
+
+
 def make_params(Ms=8.6e5, Aexch=1.3e-11, alpha=0.5, gamma=2.21e5, mu0=4e-7 * np.pi, demag=True, exchange=True,
                 external=False, hext_t=None, hext_b=None, ref_stage_time=False):
     """Material constants default to the reference's permalloy (main.cpp:107-111).
@@ -228,11 +245,12 @@ def make_params(Ms=8.6e5, Aexch=1.3e-11, alpha=0.5, gamma=2.21e5, mu0=4e-7 * np.
 
 
 M2L_AUTO, M2L_SIMT, M2L_TENSOR = 0, 1, 2
+FAR_STAGES, FAR_FUSED = 0, 1
 
 
-def make_solver(kind=SOLVER_DIRECT, order=4, leaf=0, m2l_mode=M2L_AUTO):
+def make_solver(kind=SOLVER_DIRECT, order=4, leaf=0, m2l_mode=M2L_AUTO, far_mode=FAR_STAGES):
     s = Solver()
-    s.kind, s.fmm_order, s.fmm_leaf, s.m2l_mode = kind, order, leaf, m2l_mode
+    s.kind, s.fmm_order, s.fmm_leaf, s.m2l_mode, s.far_mode = kind, order, leaf, m2l_mode, far_mode
     return s
 
 

@@ -158,3 +158,45 @@ def test_autotune_meets_target(cuda, lib, oracle_mod):
     with mmsb200.Context(grid, params, s1) as ctx:
         phi = ctx.potential_host(rho)
     assert rel_l2(phi, exact) <= 1.05 * target
+
+
+def test_autotune_on_steps(cuda, lib, oracle_mod):
+    """the step-timed search returns a solver within the target and a positive step time"""
+    import torch
+    import mmsb200
+    from mmsb200 import geometry
+    mask = geometry.disc(64, 64, 3, 30)
+    M = geometry.random_inplane(mask, 31)
+    g = oracle_mod.Grid(64, 64, 3, 5e-9, 5e-9, 5e-9)
+    rho = oracle_mod.divergence(g, M).astype(np.float32)
+    grid = mmsb200.Grid(64, 64, 3, 5e-9, 5e-9, 5e-9)
+    params = mmsb200.make_params()
+    s, ms, err = mmsb200.autotune_fmm_steps(grid, params, mask, M, 1e-13, torch.from_numpy(rho).cuda(), 5e-4, 5)
+    assert s.kind == mmsb200.SOLVER_FMM and err <= 5e-4 and ms > 0
+
+
+@pytest.mark.parametrize("X,Y,P,s", [(256, 256, 4, 4), (256, 256, 4, 8), (96, 80, 3, 4), (64, 64, 2, 4),
+                                     (200, 136, 4, 8), (128, 128, 1, 4)])
+def test_fused_far_field_is_bitwise_the_staged_one(cuda, lib, X, Y, P, s):
+    """one cooperative launch (P2M .. L2L) gives the same bits as one launch per
+    stage and level, and the fused plan runs inside the step graph"""
+    import torch
+    import mmsb200
+    from mmsb200 import geometry
+    mask = geometry.random_blocks_mask(X, Y, 3, 0.3, 4, X + Y)
+    M = geometry.random_sphere(mask, P)
+    grid = mmsb200.Grid(X, Y, 3, 5e-9, 5e-9, 5e-9)
+    rho = torch.zeros(3 * X * Y, device="cuda")
+    out = []
+    for far in (mmsb200.FAR_FUSED, mmsb200.FAR_STAGES):
+        with mmsb200.Context(grid, mmsb200.make_params(), mmsb200.make_solver(mmsb200.SOLVER_FMM, P, s,
+                                                                                mmsb200.M2L_SIMT, far)) as c:
+            c.divergence_dev(torch.from_numpy(M.astype(np.float32)).cuda(), rho)
+            phi = torch.zeros_like(rho)
+            c.potential_dev(rho, phi)
+            c.state_set(mask, M)
+            c.run_fixed(1e-13, 3)
+            c.sync()
+            out.append((phi.cpu().numpy(), c.state_get()[0]))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
