@@ -90,6 +90,7 @@ struct FmmPlan {
     TcGroup *tc_groups = nullptr;   // [8] on the device
     std::vector<TcGroup> tc_group_host;
     int tc_maxm = 0;
+    int tc_ksplit = 1;        // K split of the grouped GEMM: partial locals, summed by L2L / L2P
     float *Gn = nullptr;      // [Z][2s][2s] near-field dV/|r|
     float *Mall = nullptr;    // [boxes of all levels][NR]
     float *Lall = nullptr;    // final locals
@@ -868,15 +869,25 @@ __global__ void k_m2l_gather(const float *__restrict__ Mall, __nv_bfloat16 *__re
 
 __device__ int g_m2l_tc_err;
 
-__global__ void __launch_bounds__(128) k_m2l_gemm(const TcGroup *__restrict__ groups)
+constexpr int TC_STAGES = 4;
+
+// grouped tensor-core M2L: blockIdx.z = (parity class, parity block), x = 128
+// target rows, y = a share of K written to its own partial-local buffer
+__global__ void __launch_bounds__(128) k_m2l_gemm(const TcGroup *__restrict__ groups, int ksplit,
+                                                  long long part_stride)
 {
     extern __shared__ uint8_t raw[];
     const TcGroup g = groups[blockIdx.z];
     const int m0 = blockIdx.x * umma::BM;
     if (m0 >= g.M) return;  // before any tensor-memory allocation
+    const int ktiles = (g.K + umma::BK - 1) / umma::BK, per = (ktiles + ksplit - 1) / ksplit;
+    const int k0 = blockIdx.y * per * umma::BK;
+    const int kl = max(0, min(g.K - k0, per * umma::BK));
     uint8_t *base = (uint8_t *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
-    umma::Smem<64> &s = *reinterpret_cast<umma::Smem<64> *>(base);
-    umma::gemm_tile<64>(g.A, g.lda, g.B, g.ldb, g.C, g.ldc, g.M, g.N, g.K, m0, 0, 0, &g_m2l_tc_err, s, g.rowmap);
+    umma::Smem<64, TC_STAGES> &s = *reinterpret_cast<umma::Smem<64, TC_STAGES> *>(base);
+    umma::gemm_tile<64, TC_STAGES>(g.A + (kl > 0 ? k0 : 0), g.lda, g.B + (kl > 0 ? k0 : 0), g.ldb,
+                                   g.C + blockIdx.y * part_stride, g.ldc, g.M, g.N, kl, m0, 0, 0, &g_m2l_tc_err, s,
+                                   g.rowmap);
 }
 
 __global__ void k_build_gn(float *__restrict__ Gn, int Z, int s, double dx, double dy, double dz)
@@ -1220,7 +1231,14 @@ int fmm_plan_create(mms_ctx *ctx)
         tc_base[4] = (int)tc_rowmap.size();
         pl->tc_rows = tc_base[4];
         pl->tc_maxm = 0;
-        for (int par = 0; par < 4; par++) pl->tc_maxm = std::max(pl->tc_maxm, tc_base[par + 1] - tc_base[par]);
+        int tiles = 0;
+        for (int par = 0; par < 4; par++) {
+            pl->tc_maxm = std::max(pl->tc_maxm, tc_base[par + 1] - tc_base[par]);
+            tiles += 2 * ((tc_base[par + 1] - tc_base[par] + umma::BM - 1) / umma::BM);
+        }
+        // enough CTAs for two per SM, at least 4 K tiles each, at most NSPLIT partials
+        const int ktiles = (3 * std::max(pl->tcK[0], pl->tcK[1]) + umma::BK - 1) / umma::BK;
+        pl->tc_ksplit = std::max(1, std::min({NSPLIT, (296 + tiles - 1) / std::max(1, tiles), ktiles / 4}));
     }
     int st = MMS_OK;
     if (!st) st = upload(ctx, pl, &pl->Wt, Wt);
@@ -1297,7 +1315,7 @@ int fmm_plan_create(mms_ctx *ctx)
             MMS_CUDA_TRY(cudaMemcpyAsync(pl->tc_groups, pl->tc_group_host.data(), 8 * sizeof(TcGroup),
                                          cudaMemcpyHostToDevice, ctx->stream));
             MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2l_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)(sizeof(umma::Smem<64>) + 1024)));
+                                              (int)(sizeof(umma::Smem<64, TC_STAGES>) + 1024)));
         }
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Mall, 0, ncoef * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->Lall, 0, ncoef * sizeof(float), ctx->stream));
@@ -1401,7 +1419,7 @@ static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
     FmmPlan *pl = ctx->fmm;
     const FmmDev &f = pl->d;
     const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
-    const int nsplit = (pl->m2l_resident || pl->m2l_tc) ? 1 : NSPLIT;
+    const int nsplit = pl->m2l_tc ? pl->tc_ksplit : (pl->m2l_resident ? 1 : NSPLIT);
     const float *Lpar = f.L > 2 ? pl->Lall + pl->lev_off[f.L - 1] * f.NR : nullptr;
     MMS_TRY(l2p_launch(f, nbx, nby, pl->near, pl->Lpart + pl->lev_off[f.L] * f.NR, Lpar, pl->Tl2l, pl->Vt, phi,
                        pl->nbox_total * f.NR, nsplit, ctx->stream));
@@ -1423,7 +1441,7 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     const int thr = ((f.NR + 31) / 32) * 32;
     const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
     const int KT = ((f.NR + 31) / 32) * 32;
-    const int nsplit = (pl->m2l_resident || pl->m2l_tc) ? 1 : NSPLIT;
+    const int nsplit = pl->m2l_tc ? pl->tc_ksplit : (pl->m2l_resident ? 1 : NSPLIT);
     if (stage < 4 && !far) return MMS_OK;
     switch (stage) {
     case 0: {
@@ -1450,8 +1468,9 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
                                                                       pl->tc_rowinfo, pl->lev_dev, f, pl->tcK[0],
                                                                       pl->tcK[1], pl->tcNBp[0], pl->tcNBp[1]);
             MMS_LAUNCH_CHECK(ctx);
-            k_m2l_gemm<<<dim3(div_up(pl->tc_maxm, umma::BM), 1, 8), 128, sizeof(umma::Smem<64>) + 1024,
-                         ctx->stream>>>(pl->tc_groups);
+            k_m2l_gemm<<<dim3(div_up(pl->tc_maxm, umma::BM), pl->tc_ksplit, 8), 128,
+                         sizeof(umma::Smem<64, TC_STAGES>) + 1024, ctx->stream>>>(pl->tc_groups, pl->tc_ksplit,
+                                                                                 part_stride);
             MMS_LAUNCH_CHECK(ctx);
             break;
         }

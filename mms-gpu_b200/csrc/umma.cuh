@@ -114,27 +114,51 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float v[16])
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// shared memory of one CTA: STAGES x (A tile 16 KB + B tile BN x 128 B), 1024-aligned
-template <int BN>
+// shared memory of one CTA: S x (A tile 16 KB + B tile BN x 128 B), 1024-aligned
+template <int BN, int S = STAGES>
 struct Smem {
-    alignas(1024) uint8_t a[STAGES][BM * 128];
-    alignas(1024) uint8_t b[STAGES][BN * 128];
-    uint64_t done[STAGES];   // MMA of this stage finished (stage may be refilled)
+    alignas(1024) uint8_t a[S][BM * 128];
+    alignas(1024) uint8_t b[S][BN * 128];
+    uint64_t done[S];        // MMA of this stage finished (stage may be refilled)
     uint32_t tmem;           // allocated tensor-memory address
     int err;
 };
+
+__device__ __forceinline__ void cp_async_wait_pending(int pending)
+{
+    // wait until at most `pending` committed groups are still in flight
+    if (pending >= 6)
+        asm volatile("cp.async.wait_group 6;\n" ::: "memory");
+    else if (pending == 5)
+        asm volatile("cp.async.wait_group 5;\n" ::: "memory");
+    else if (pending == 4)
+        asm volatile("cp.async.wait_group 4;\n" ::: "memory");
+    else if (pending == 3)
+        asm volatile("cp.async.wait_group 3;\n" ::: "memory");
+    else if (pending == 2)
+        asm volatile("cp.async.wait_group 2;\n" ::: "memory");
+    else if (pending == 1)
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    else
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 
 // One 128 x BN tile of C.  A is M x K (lda), B is N x K (ldb), both BF16 with
 // K contiguous; rows beyond M / N and columns beyond K read as zero.
 // beta != 0: C += A B^T, else C = A B^T.  err: set to 1 on a barrier timeout.
 // rowmap (may be NULL): row r of the tile result goes to C row rowmap[r].
-template <int BN>
+// S pipeline stages (S - 1 tiles of cp.async loads in flight ahead of the
+// tensor core); NT = 128 or 256 threads (256: two warps per TMEM lane quarter,
+// splitting the loads and the epilogue's columns).
+template <int BN, int S = STAGES, int NT = 128>
 __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __nv_bfloat16 *__restrict__ B, int ldb,
                           float *__restrict__ C, int ldc, int M, int N, int K, int m0, int n0, int beta,
-                          int *__restrict__ err, Smem<BN> &s, const int *__restrict__ rowmap = nullptr)
+                          int *__restrict__ err, Smem<BN, S> &s, const int *__restrict__ rowmap = nullptr)
 {
     static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN must be a power of two in [32, 256]");
-    const int tid = threadIdx.x;  // 128 threads
+    static_assert(S >= 2 && S <= 8, "2..8 stages");
+    static_assert(NT == 128 || NT == 256, "128 or 256 threads");
+    const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&s.tmem)),
@@ -143,7 +167,7 @@ __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
     if (tid == 0) {
-        for (int i = 0; i < STAGES; i++) mbar_init(&s.done[i]);
+        for (int i = 0; i < S; i++) mbar_init(&s.done[i]);
         s.err = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
@@ -157,13 +181,13 @@ __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __
     auto load_stage = [&](int st, int kt) {
         const int k0 = kt * BK;
         const uint32_t sa = smem_u32(s.a[st]), sb = smem_u32(s.b[st]);
-        for (int i = tid; i < BM * 8; i += 128) {
+        for (int i = tid; i < BM * 8; i += NT) {
             const int r = i >> 3, c = i & 7;
             const int gr = m0 + r, gk = k0 + c * 8;
             const bool ok = gr < M && gk < K;  // K is a multiple of 8 (16-byte rows)
             cp_async16(sa + sw128_off(r, c), ok ? (const void *)(A + (long long)gr * lda + gk) : (const void *)A, ok);
         }
-        for (int i = tid; i < BN * 8; i += 128) {
+        for (int i = tid; i < BN * 8; i += NT) {
             const int r = i >> 3, c = i & 7;
             const int gr = n0 + r, gk = k0 + c * 8;
             const bool ok = gr < N && gk < K;
@@ -172,25 +196,14 @@ __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
 
-    uint32_t phase[STAGES] = {0, 0};
     bool ok = true;
-    if (nk > 0) load_stage(0, 0);
+    int issued = 0;
+    for (; issued < S - 1 && issued < nk; issued++) load_stage(issued % S, issued);
     for (int kt = 0; kt < nk && ok; kt++) {
-        const int st = kt % STAGES;
-        if (kt + 1 < nk) {
-            const int nst = (kt + 1) % STAGES;
-            if (kt + 1 >= STAGES) {  // the MMAs that read stage nst (tile kt+1-STAGES) must be done
-                ok = mbar_wait(&s.done[nst], phase[nst]);
-                phase[nst] ^= 1;
-            }
-            if (ok) load_stage(nst, kt + 1);
-            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        }
+        const int st = kt % S;
+        cp_async_wait_pending(issued - kt - 1);  // tile kt has landed
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
-        if (!ok) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
             const uint32_t sa = smem_u32(s.a[st]), sb = smem_u32(s.b[st]);
@@ -200,28 +213,31 @@ __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __
             mma_commit(&s.done[st]);
         }
         __syncwarp();
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // no copy may still be in flight at exit
-    // wait for the last commit of every stage still pending
-    if (ok && nk > 0) {
-        for (int kt = (nk > STAGES ? nk - STAGES : 0); kt < nk; kt++) {
-            const int st = kt % STAGES;
-            if (!mbar_wait(&s.done[st], phase[st])) {
-                ok = false;
-                break;
+        if (issued < nk) {
+            // the stage to refill was read by the MMAs of tile kt - 1
+            if (kt >= 1) ok = mbar_wait(&s.done[(kt - 1) % S], (uint32_t)(((kt - 1) / S) & 1));
+            if (ok) {
+                load_stage(issued % S, issued);
+                issued++;
             }
-            phase[st] ^= 1;
         }
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // no copy may still be in flight at exit
+    // the last commit covers every earlier MMA of this thread
+    if (ok && nk > 0) ok = mbar_wait(&s.done[(nk - 1) % S], (uint32_t)(((nk - 1) / S) & 1));
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    // epilogue: warp w reads accumulator rows 32 (w % 4) .. +31 (its TMEM lane
+    // quarter); with 256 threads warps 4..7 take the upper half of the columns
+    const int quarter = warp & 3;
+    const int cbeg = (NT == 256) ? (warp >> 2) * (BN / 2) : 0;
+    const int cend = (NT == 256) ? cbeg + BN / 2 : BN;
     if (!ok) {
         if (lane == 0) atomicExch(err, 1);
     } else if (nk > 0) {
-        // epilogue: warp w owns accumulator rows 32w .. 32w+31 (TMEM lanes)
-        const int row = m0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < BN; c0 += 16) {
+        const int row = m0 + quarter * 32 + lane;
+        for (int c0 = cbeg; c0 < cend; c0 += 16) {
             float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, v);
             if (row < M) {
                 const long long crow_i = rowmap ? (long long)rowmap[row] : (long long)row;
                 float *crow = C + crow_i * ldc + n0 + c0;
@@ -231,10 +247,10 @@ __device__ void gemm_tile(const __nv_bfloat16 *__restrict__ A, int lda, const __
             }
         }
     } else if (!beta) {
-        const int row = m0 + warp * 32 + lane;
+        const int row = m0 + quarter * 32 + lane;
         if (row < M) {
             const long long crow_i = rowmap ? (long long)rowmap[row] : (long long)row;
-            for (int c = 0; c < BN && n0 + c < N; c++) C[crow_i * ldc + n0 + c] = 0.f;
+            for (int c = cbeg; c < cend && n0 + c < N; c++) C[crow_i * ldc + n0 + c] = 0.f;
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
