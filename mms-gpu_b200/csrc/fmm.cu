@@ -189,21 +189,66 @@ __device__ __forceinline__ void p2m_item(const float *__restrict__ rho, const fl
     __syncthreads();
 }
 
-// P2M: CTA = one item (BB leaf boxes of one row)
-__global__ void __launch_bounds__(128) k_p2m_row(const float *__restrict__ rho, const float *__restrict__ Wg,
-                                                 float *__restrict__ Mleaf, FmmDev f, int wsm)
+__device__ __forceinline__ void m2m_item(float *__restrict__ Mall, const float *Ts, float *Mc, float *red,
+                                         long long off_p, long long off_c, int np, int box, const FmmDev &f, int t,
+                                         int KT, bool valid);
+
+// P2M: CTA = one item (BB leaf boxes of one row).  With up != 0 (NR <= 32)
+// the CTA takes two leaf rows (both in parallel, thread per (row, box,
+// coefficient)) and then forms their BB/2 parents (the M2M of level L-1) with
+// one 4 KT-thread group per parent, reading the children it just wrote; 512
+// threads.  Per output the same summation order as p2m_item / m2m_item.
+// Shared memory: charges [rows][C][BB], W [C][NR] when wsm, then (up) the M2M
+// operators and the per-parent M2M scratch.
+__global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, const float *__restrict__ Wg,
+                                                 float *__restrict__ Mall, long long off_leaf, FmmDev f, int wsm,
+                                                 int up, const float *__restrict__ Tm2m, long long off_par)
 {
     pdl_begin();
-    extern __shared__ __align__(16) float q[];  // [C][BB], then W [C][NR] when wsm
+    extern __shared__ __align__(16) float q[];
+    const int rows = up ? 2 : 1;
     const float *Wt = Wg;
+    float *tail = q + rows * f.C * BB;
     if (wsm) {
-        float *Ws = q + f.C * BB;
+        float *Ws = tail;
         const int n = f.C * f.NR;
         for (int i = threadIdx.x * 4; i < n; i += blockDim.x * 4)
             *reinterpret_cast<float4 *>(&Ws[i]) = __ldg(reinterpret_cast<const float4 *>(&Wg[i]));
         Wt = Ws;
+        tail += n;
     }
-    p2m_item(rho, Wt, q, Mleaf, f, blockIdx.y, blockIdx.x * BB);
+    float *Mleaf = Mall + off_leaf * f.NR;
+    const int bx0 = blockIdx.x * BB;
+    if (!up) {
+        p2m_item(rho, Wt, q, Mleaf, f, blockIdx.y, bx0);
+        return;
+    }
+    const int NE = f.NE, NO = f.NR - f.NE, s = f.s, CB = f.C * BB;
+    const int tsz = 4 * (NE * NE + NO * NO);
+    const int KT = ((f.NR + 31) / 32) * 32;
+    float *Ts = tail, *scr = Ts + tsz;
+    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tm2m[i]));
+    for (int i = threadIdx.x; i < 2 * CB; i += blockDim.x) {
+        const int r = i / CB, j = i % CB, b = j % BB, c = j / BB;
+        const int x = (bx0 + b) * s + c % s, y = (2 * blockIdx.y + r) * s + (c / s) % s, z = c / (s * s);
+        q[i] = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 2 * BB * f.NR; e += blockDim.x) {
+        const int r = e / (BB * f.NR), rem = e % (BB * f.NR), b = rem / f.NR, k = rem % f.NR;
+        const float *qr = q + r * CB;
+        float acc = 0.f;
+#pragma unroll 4
+        for (int c = 0; c < f.C; c++) acc = fmaf(Wt[(long long)c * f.NR + k], qr[c * BB + b], acc);
+        if (bx0 + b < f.nb) Mleaf[((long long)(2 * blockIdx.y + r) * f.nb + bx0 + b) * f.NR + k] = acc;
+    }
+    __syncthreads();
+    const int np = f.nb >> 1;
+    const int grp = threadIdx.x / (4 * KT), t = threadIdx.x % (4 * KT);
+    const int pc = (bx0 >> 1) + grp;
+    float *Mc = scr + grp * (4 * f.NR + 4 * KT), *red = Mc + 4 * f.NR;
+    m2m_item(Mall, Ts, Mc, red, off_par, off_leaf, np, blockIdx.y * np + pc, f, t, KT, grp < BB / 2 && pc < np);
 }
 
 // M2M: CTA per parent box, thread per (child c, output coefficient k).  The
@@ -745,29 +790,67 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
 // k_l2p: leaf locals (the leaf level's L2L: NSPLIT-summed M2L partials plus
 // the L2L of the parent's final local, none when the leaf level is 2), then
 // phi = near field + sum_k V[k][cell] L[k].  Same thread layout as k_p2p.
+// The parents' final locals (level L-1) come, by pmode:
+//   0  none (leaf level 2)
+//   1  ready in Lpar (an L2L pass formed them)
+//   2  formed here: L2L of the grandparents' final locals (Lgp, level L-2)
+//      plus the parents' M2L partials (Lpp), the order of the L2L pass
+//   3  formed here from the parents' partials alone (parent level 2)
 template <int S, int BB>
 __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, const float *__restrict__ Lpart_leaf,
                                               const float *__restrict__ Lpar, const float *__restrict__ Tl2l,
                                               const float *__restrict__ Vt, float *__restrict__ phi, FmmDev f,
-                                              long long part_stride, int nsplit)
+                                              long long part_stride, int nsplit, int pmode,
+                                              const float *__restrict__ Lgp, const float *__restrict__ Lpp)
 {
     pdl_begin();
     extern __shared__ __align__(16) float sl[];
     const int Z = f.Z;
     const int NE = f.NE, NO = f.NR - f.NE;
+    constexpr int GB = BB >= 4 ? BB / 4 : 1;          // grandparents under the CTA's BB leaves
     float *Ts = sl;                                   // L2L operator blocks
     float *Lb = Ts + 4 * (NE * NE + NO * NO);         // [BB][NR] leaf locals
     float *Lp = Lb + BB * f.NR;                       // [BB/2][NR] parent locals
+    float *Lg = Lp + (BB / 2) * f.NR;                 // [GB][NR] grandparent locals
     const int by = blockIdx.y, bx0 = blockIdx.x * BB;
-    const int haspar = f.L > 2;
+    const int haspar = pmode != 0;
+    const int np = f.nb >> 1, prow = by >> 1;
     if (haspar) {
         const int tsz = 4 * (NE * NE + NO * NO);
         for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
             *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tl2l[i]));
-        const int np = f.nb >> 1;
+    }
+    if (pmode == 1) {
         for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
             const int pb = (bx0 >> 1) + i / f.NR;
-            Lp[i] = (pb < np) ? Lpar[((long long)(by >> 1) * np + pb) * f.NR + i % f.NR] : 0.f;
+            Lp[i] = (pb < np) ? Lpar[((long long)prow * np + pb) * f.NR + i % f.NR] : 0.f;
+        }
+    } else if (pmode >= 2) {
+        const int ng = np >> 1, g0 = bx0 >> 2;
+        if (pmode == 2)
+            for (int i = threadIdx.x; i < GB * f.NR; i += blockDim.x) {
+                const int gc = g0 + i / f.NR;
+                Lg[i] = (gc < ng) ? Lgp[((long long)(prow >> 1) * ng + gc) * f.NR + i % f.NR] : 0.f;
+            }
+        __syncthreads();
+        for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
+            const int pc = (bx0 >> 1) + i / f.NR, k = i % f.NR;
+            float v = 0.f;
+            if (pc < np) {
+                if (pmode == 2) {
+                    const int c = (pc & 1) | ((prow & 1) << 1);
+                    const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+                    const float *T = Ts + blk_base(c, NE, NO, blk);
+                    const float *lg = Lg + ((pc >> 1) - g0) * f.NR + boff;
+                    float acc = 0.f;
+#pragma unroll 8
+                    for (int j = 0; j < NB; j++) acc = fmaf(T[j * NB + kk], lg[j], acc);
+                    v = acc;
+                }
+                const long long pbox = (long long)prow * np + pc;
+                for (int q = 0; q < nsplit; q++) v += Lpp[q * part_stride + pbox * f.NR + k];
+            }
+            Lp[i] = v;
         }
     }
     __syncthreads();
@@ -938,7 +1021,8 @@ size_t l2p_smem(const FmmDev &f)
 {
     const int B = leaf_bb(f.s);
     const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
-    return (tsz + (size_t)B * f.NR + (size_t)(B / 2) * f.NR) * sizeof(float);
+    const int GB = B >= 4 ? B / 4 : 1;
+    return (tsz + (size_t)B * f.NR + (size_t)(B / 2) * f.NR + (size_t)GB * f.NR) * sizeof(float);
 }
 
 #define MMS_LEAF_CASES(X) X(2, 8) X(4, 8) X(8, 4) X(16, 4)
@@ -973,10 +1057,11 @@ int p2p_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float 
 }
 
 int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float *Lpart_leaf, const float *Lpar,
-               const float *Tl2l, const float *Vt, float *phi, long long part_stride, int nsplit, cudaStream_t st)
+               const float *Tl2l, const float *Vt, float *phi, long long part_stride, int nsplit, int pmode,
+               const float *Lgp, const float *Lpp, cudaStream_t st)
 {
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
-#define X(S_, B_) if (f.s == S_) { MMS_CUDA_TRY(launch_k(k_l2p<S_, B_>, grid, dim3(leaf_threads(f)), l2p_smem(f), st, near, Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit)); return MMS_OK; }
+#define X(S_, B_) if (f.s == S_) { MMS_CUDA_TRY(launch_k(k_l2p<S_, B_>, grid, dim3(leaf_threads(f)), l2p_smem(f), st, near, Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp)); return MMS_OK; }
     MMS_LEAF_CASES(X)
 #undef X
     mms_set_error("no leaf kernel for side %d", f.s);
@@ -1331,9 +1416,8 @@ int fmm_plan_create(mms_ctx *ctx)
     if (pl->m2l_resident && NR <= 30 && leaf_threads(f) > 0 && f.L >= 2 && ctx->s.far_mode == 1)
         MMS_TRY(far_prepare(ctx, pl));
     {
-        const size_t pm = (size_t)f.C * (BB + f.NR) * sizeof(float);
-        if (pm > 48 * 1024 && pm <= 160 * 1024)
-            MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pm));
+        // P2M with W staged and the fused parent M2M: at most 160 KB
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     }
     {
         const size_t tsz = 4 * cstride;
@@ -1412,6 +1496,13 @@ void fmm_plan_destroy(mms_ctx *ctx)
 
 size_t fmm_plan_bytes(const mms_ctx *ctx) { return ctx->fmm ? ctx->fmm->bytes : 0; }
 
+// the per-stage path forms level L-1's locals inside L2P (one launch fewer
+// after the M2L) when the tree has a level L-1 >= 2 and the leaf kernels
+// exist, and level L-1's multipoles inside P2M when also NR <= 32 (P <= 4:
+// one 128-thread group per parent, 512 threads)
+static int l2p_up(const FmmPlan *pl) { return pl->d.L >= 3 && leaf_threads(pl->d) > 0 && !pl->far_fused; }
+static int p2m_up(const FmmPlan *pl) { return l2p_up(pl) && pl->d.NR <= 32; }
+
 // L2P of the far field onto the near field already in pl->near
 static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
 {
@@ -1421,11 +1512,16 @@ static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
     const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
     const int nsplit = pl->m2l_tc ? pl->tc_ksplit : (pl->m2l_resident ? 1 : NSPLIT);
     const float *Lpar = f.L > 2 ? pl->Lall + pl->lev_off[f.L - 1] * f.NR : nullptr;
+    // parents' locals: ready (an L2L pass made level L-1) or formed in the leaf kernel
+    const int pmode = f.L <= 2 ? 0 : (!l2p_up(pl) ? 1 : (f.L - 1 >= 3 ? 2 : 3));
+    const float *Lgp = f.L >= 4 ? pl->Lall + pl->lev_off[f.L - 2] * f.NR : nullptr;
+    const float *Lpp = f.L > 2 ? pl->Lpart + pl->lev_off[f.L - 1] * f.NR : nullptr;
     MMS_TRY(l2p_launch(f, nbx, nby, pl->near, pl->Lpart + pl->lev_off[f.L] * f.NR, Lpar, pl->Tl2l, pl->Vt, phi,
-                       pl->nbox_total * f.NR, nsplit, ctx->stream));
+                       pl->nbox_total * f.NR, nsplit, pmode, Lgp, Lpp, ctx->stream));
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
+
 
 // One stage of the FMM potential: 0 P2M, 1 M2M (all levels), 2 M2L (all
 // levels), 3 L2L (all levels, with the M2L partial sums), 4 L2P + P2P.  Every
@@ -1446,15 +1542,22 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     switch (stage) {
     case 0: {
         const long long leaf_off = pl->lev_off[f.L];
-        const int wsm = (f.C * f.NR) % 4 == 0 && (size_t)f.C * (BB + f.NR) * sizeof(float) <= 160 * 1024;
-        MMS_CUDA_TRY(launch_k(k_p2m_row, dim3(div_up(nbx, BB), nby), dim3(128),
-                              (size_t)f.C * (BB + (wsm ? f.NR : 0)) * sizeof(float), ctx->stream, rho,
-                              (const float *)pl->Wt, pl->Mall + leaf_off * f.NR, f, wsm));
+        const int up = p2m_up(pl);
+        const int rows = up ? 2 : 1;
+        const size_t extra = up ? tsz + (BB / 2) * (4 * (size_t)f.NR + 4 * (size_t)KT) : 0;
+        const int wsm =
+            (f.C * f.NR) % 4 == 0 && ((size_t)f.C * (rows * BB + f.NR) + extra) * sizeof(float) <= 160 * 1024;
+        const size_t smem = ((size_t)f.C * (rows * BB + (wsm ? f.NR : 0)) + extra) * sizeof(float);
+        MMS_CUDA_TRY(launch_k(k_p2m_row, dim3(div_up(nbx, BB), up ? div_up(nby, 2) : nby),
+                              dim3(up ? (BB / 2) * 4 * KT : 128), smem, ctx->stream, rho, (const float *)pl->Wt,
+                              pl->Mall, leaf_off, f, wsm, up, (const float *)pl->Tm2m,
+                              up ? pl->lev_off[f.L - 1] : 0LL));
         MMS_LAUNCH_CHECK(ctx);
         break;
     }
     case 1:
-        for (int l = f.L - 1; l >= 2; l--) {
+        // level L-1 is formed inside P2M when p2m_up()
+        for (int l = f.L - 1 - p2m_up(pl); l >= 2; l--) {
             const int np = 1 << l;
             MMS_CUDA_TRY(launch_k(k_m2m_c, dim3(np * np), dim3(4 * KT),
                                   (tsz + 4 * (size_t)f.NR + 4 * (size_t)KT) * sizeof(float), ctx->stream, pl->Mall,
@@ -1493,7 +1596,7 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         // level 2 from its M2L partials, levels 3 .. L-1 one launch each; the
         // leaf level is formed inside the leaf kernel (or by k_l2l_c for the
         // generic leaf kernel)
-        const int lend = leaf_threads(f) > 0 ? f.L - 1 : f.L;
+        const int lend = leaf_threads(f) > 0 ? f.L - 1 - l2p_up(pl) : f.L;
         if (lend >= 2) {
             MMS_CUDA_TRY(launch_k(k_l2l_c, dim3(16), dim3(thr), 0, ctx->stream, pl->Lall,
                                   (const float *)pl->Lpart, (const float *)pl->Tl2l, 0LL, pl->lev_off[2], 4, 0,

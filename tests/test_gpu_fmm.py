@@ -176,7 +176,8 @@ def test_autotune_on_steps(cuda, lib, oracle_mod):
 
 
 @pytest.mark.parametrize("X,Y,P,s", [(256, 256, 4, 4), (256, 256, 4, 8), (96, 80, 3, 4), (64, 64, 2, 4),
-                                     (200, 136, 4, 8), (128, 128, 1, 4)])
+                                     (200, 136, 4, 8), (128, 128, 1, 4), (32, 32, 4, 4), (16, 12, 4, 4),
+                                     (72, 40, 4, 4)])
 def test_fused_far_field_is_bitwise_the_staged_one(cuda, lib, X, Y, P, s):
     """one cooperative launch (P2M .. L2L) gives the same bits as one launch per
     stage and level, and the fused plan runs inside the step graph"""
