@@ -460,16 +460,18 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
 
 
 def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):
-    """FMM roofline for its largest single kernel, the M2L (one launch per
-    evaluation, all levels; the largest share of the ncu launch list).  Each
-    stage is timed live with CUDA events over back-to-back re-launches on the
-    library's stream; achieved = the M2L's algorithmic flops (NE^2 + NO^2
-    multiply-adds per interaction-list box pair) over its time, against the
-    measured FP32 FMA peak.  All stage times and flops are reported beside it."""
+    """FMM roofline for its dominant stage: every stage is timed live with CUDA
+    events over back-to-back re-launches on the library's stream, and the
+    stage with the largest time is reported (at P = 4, leaf 8: the near field
+    k_p2p plus k_l2p; at leaf 4: the M2L).  achieved = that stage's
+    algorithmic flops (near field: 2 per target-source pair plus 2 NR per
+    target; M2L: 2 (NE^2 + NO^2) per interaction-list box pair) over its time,
+    against the measured FP32 FMA peak.  All stage times and flops are
+    reported beside it; traffic is the committed ncu capture of that stage."""
     import mmsb200
     st = mmsb200.fmm_stats(ctx)
     times = mmsb200.fmm_stage_times(ctx, rho, phi, reps=20)
-    dom = "m2l"
+    dom = max(times, key=lambda k: times[k])
     roof = {"kernel": f"{STAGE_KERNEL[dom]} (FMM stage {dom})", "bound": "fp32", "peak": fma_peak,
             "unit": "TFLOP/s",
             "peak_source": "measured FP32 FMA microbenchmark (mms_diag_fma_tflops), of measured"}
@@ -479,7 +481,7 @@ def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):
     roof["stage_flops"] = st["stage_flops"]
     roof["whole_potential_tflops"] = st["flops"] / (sum(times.values()) * 1e-3) / 1e12
     roof["plan"] = {k: st[k] for k in ("levels", "leaf", "order", "p2p_pairs", "m2l_pairs")}
-    roof["traffic"] = profile_traffic(f"fmm_{dom}_256x256x3")
+    roof["traffic"] = profile_traffic(f"fmm_{dom}_256x256x3_P{st['order']}_leaf{st['leaf']}")
     return roof
 
 

@@ -1113,6 +1113,8 @@ int m2l_res_launch(const FmmDev &f, int nitems, const float *Mall, float *Lout, 
 
 int fmm_default_leaf(int P, int X, int Y);
 int far_prepare(mms_ctx *ctx, FmmPlan *pl);
+static int l2p_up(const FmmPlan *pl);
+static int p2m_up(const FmmPlan *pl);
 
 int fmm_plan_create(mms_ctx *ctx)
 {
@@ -1465,6 +1467,26 @@ int fmm_plan_create(mms_ctx *ctx)
             pairs += (long long)tx * ty * Z * sx * sy * Z;
         }
     pl->stage_flops[4] += 2.0 * pairs;
+    // attribute the levels the leaf kernels form to the stage that runs them:
+    // the leaf-level L2L (and level L-1's, l2p_up) to L2P, level L-1's M2M
+    // (p2m_up) to P2M
+    if (leaf_threads(f) > 0 && f.L >= 2) {
+        const double leafl2l = 2.0 * (double)(1 << f.L) * (1 << f.L) * blk2;
+        if (f.L >= 3) {
+            pl->stage_flops[3] -= leafl2l;
+            pl->stage_flops[4] += leafl2l;
+        }
+        if (l2p_up(pl) && f.L - 1 >= 3) {
+            const double m = 2.0 * (double)(1 << (f.L - 1)) * (1 << (f.L - 1)) * blk2;
+            pl->stage_flops[3] -= m;
+            pl->stage_flops[4] += m;
+        }
+        if (p2m_up(pl)) {
+            const double m = 2.0 * 4.0 * (double)(1 << (f.L - 1)) * (1 << (f.L - 1)) * blk2;
+            pl->stage_flops[1] -= m;
+            pl->stage_flops[0] += m;
+        }
+    }
     if (f.L < 2)
         for (int i = 0; i < 4; i++) pl->stage_flops[i] = 0;
     if (f.L < 2) pl->stage_flops[4] = 2.0 * pairs;
