@@ -716,12 +716,14 @@ __global__ void __launch_bounds__(32 * RES_WARPS) k_far(const float *__restrict_
 // side stream concurrently with the far-field chain (P2M .. L2L); the L2P
 // kernel joins the two.
 //
-// k_p2p: exact near field.  CTA = BB leaf boxes of one row; thread = (box,
-// target row y, layer z) holding the S targets of its row in registers.  For
-// every source row of the 3x3 leaf neighbourhood the thread loads the 3S
-// charges and the 2S-entry near-field row G[|dz|][|dy|][.] into registers and
-// does 3S x S FMAs with compile-time indices |S + i - j|.
-template <int S, int BB>
+// k_p2p: exact near field.  CTA = BB leaf boxes of one row; G thread groups,
+// each thread = (group, box, target row y, layer z) holding the S targets of
+// its row in registers.  Group g takes the g-th third of the neighbourhood's
+// source rows (G = 3: one source box row each); for every source row the
+// thread loads the 3S charges and the 2S-entry near-field row G[|dz|][|dy|][.]
+// into registers and does 3S x S FMAs with compile-time indices |S + i - j|.
+// The groups' partial sums are added in group order through shared memory.
+template <int S, int BB, int G>
 __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, const float *__restrict__ Gn,
                                               float *__restrict__ out, FmmDev f)
 {
@@ -739,15 +741,17 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
     }
     for (int i = threadIdx.x; i < Z * 4 * S * S; i += blockDim.x) g[i] = Gn[i];
     __syncthreads();
-    const int t = threadIdx.x;
+    const int nt = BB * S * Z;
+    const int grp = threadIdx.x / nt, t = threadIdx.x % nt;
     const int b = t / (S * Z), r = t % (S * Z);
     const int ly = r % S, lz = r / S;
     float acc[S];
 #pragma unroll
     for (int i = 0; i < S; i++) acc[i] = 0.f;
+    constexpr int RG = 3 * S / G;  // source rows per group
     for (int zs = 0; zs < Z; zs++) {
         const int dz = abs(zs - lz);
-        for (int ys = 0; ys < 3 * S; ys++) {
+        for (int ys = grp * RG; ys < (grp + 1) * RG; ys++) {
             const int dy = abs(ys - ly - S);
             const float *grow = g + (dz * 2 * S + dy) * 2 * S;
             const float *qrow = qn + (zs * 3 * S + ys) * W + b * S;
@@ -778,6 +782,17 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
                 }
         }
     }
+    if constexpr (G > 1) {
+        float *red = g + Z * 4 * S * S;  // [G-1][S][nt]
+        if (grp > 0)
+#pragma unroll
+            for (int i = 0; i < S; i++) red[((grp - 1) * S + i) * nt + t] = acc[i];
+        __syncthreads();
+        if (grp > 0) return;
+        for (int gg = 1; gg < G; gg++)
+#pragma unroll
+            for (int i = 0; i < S; i++) acc[i] += red[((gg - 1) * S + i) * nt + t];
+    }
     const int y = by * S + ly;
     if (bx0 + b >= f.nb || y >= f.Y) return;
 #pragma unroll
@@ -796,7 +811,7 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
 //   2  formed here: L2L of the grandparents' final locals (Lgp, level L-2)
 //      plus the parents' M2L partials (Lpp), the order of the L2L pass
 //   3  formed here from the parents' partials alone (parent level 2)
-template <int S, int BB>
+template <int S, int BB, int G>
 __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, const float *__restrict__ Lpart_leaf,
                                               const float *__restrict__ Lpar, const float *__restrict__ Tl2l,
                                               const float *__restrict__ Vt, float *__restrict__ phi, FmmDev f,
@@ -871,19 +886,22 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
         Lb[i] = v;
     }
     __syncthreads();
-    const int t = threadIdx.x;
+    // G thread groups: group g evaluates coefficients [k0, k1) of every target
+    const int nt = BB * S * Z;
+    const int grp = threadIdx.x / nt, t = threadIdx.x % nt;
     const int b = t / (S * Z), r = t % (S * Z);
     const int ly = r % S, lz = r / S;
     const int y = by * S + ly;
-    if (bx0 + b >= f.nb || y >= f.Y) return;
+    const bool valid = bx0 + b < f.nb && y < f.Y;
     const long long row = ((long long)lz * f.Y + y) * f.X + (long long)(bx0 + b) * S;
     float acc[S];
 #pragma unroll
-    for (int i = 0; i < S; i++) acc[i] = ((bx0 + b) * S + i < f.X) ? near[row + i] : 0.f;
+    for (int i = 0; i < S; i++) acc[i] = (valid && grp == 0 && (bx0 + b) * S + i < f.X) ? near[row + i] : 0.f;
     const float *Lbb = Lb + b * f.NR;
     const int c0 = lz * S * S + ly * S;
+    const int k0 = grp * f.NR / G, k1 = valid ? (grp + 1) * f.NR / G : k0;
 #pragma unroll 4
-    for (int k = 0; k < f.NR; k++) {
+    for (int k = k0; k < k1; k++) {
         const float lk = Lbb[k];
         const float *vrow = Vt + (long long)k * f.C + c0;
         if constexpr (S % 4 == 0) {
@@ -900,6 +918,19 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
             for (int i = 0; i < S; i++) acc[i] = fmaf(__ldg(&vrow[i]), lk, acc[i]);
         }
     }
+    if constexpr (G > 1) {
+        __syncthreads();  // the leaf locals are no longer read: Lb .. becomes [G-1][S][nt]
+        float *red = Lb;
+        if (grp > 0)
+#pragma unroll
+            for (int i = 0; i < S; i++) red[((grp - 1) * S + i) * nt + t] = acc[i];
+        __syncthreads();
+        if (grp > 0) return;
+        for (int gg = 1; gg < G; gg++)
+#pragma unroll
+            for (int i = 0; i < S; i++) acc[i] += red[((gg - 1) * S + i) * nt + t];
+    }
+    if (!valid) return;
 #pragma unroll
     for (int i = 0; i < S; i++)
         if ((bx0 + b) * S + i < f.X) phi[row + i] = acc[i];
@@ -1011,10 +1042,19 @@ int leaf_threads(const FmmDev &f)
     return t <= 512 ? t : 0;
 }
 
+// thread groups per leaf box in k_l2p (on the critical path after the join):
+// 3 while the CTA stays <= 512 threads
+int leaf_groups(const FmmDev &f) { return 3 * leaf_threads(f) <= 512 ? 3 : 1; }
+// in k_p2p, which runs beside the far-field chain: wider CTAs pay off while the
+// near field is small (leaf <= 4); at leaf 8 they crowd the far chain's kernels
+// off the SMs (measured: 3530 -> 3262 steps/s at 256 x 256 x 3)
+int p2p_groups(const FmmDev &f) { return f.s <= 4 ? leaf_groups(f) : 1; }
+
 size_t p2p_smem(const FmmDev &f)
 {
     const int S = f.s, B = leaf_bb(S), W = (B + 2) * S;
-    return ((size_t)f.Z * 3 * S * W + (size_t)f.Z * 4 * S * S) * sizeof(float);
+    return ((size_t)f.Z * 3 * S * W + (size_t)f.Z * 4 * S * S +
+            (size_t)(p2p_groups(f) - 1) * S * leaf_threads(f)) * sizeof(float);
 }
 
 size_t l2p_smem(const FmmDev &f)
@@ -1022,7 +1062,10 @@ size_t l2p_smem(const FmmDev &f)
     const int B = leaf_bb(f.s);
     const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
     const int GB = B >= 4 ? B / 4 : 1;
-    return (tsz + (size_t)B * f.NR + (size_t)(B / 2) * f.NR + (size_t)GB * f.NR) * sizeof(float);
+    // after the leaf locals are consumed, the area from Lb on holds the groups' partial sums
+    const size_t locals = (size_t)B * f.NR + (size_t)(B / 2) * f.NR + (size_t)GB * f.NR;
+    const size_t partial = (size_t)(leaf_groups(f) - 1) * f.s * leaf_threads(f);
+    return (tsz + std::max(locals, partial)) * sizeof(float);
 }
 
 #define MMS_LEAF_CASES(X) X(2, 8) X(4, 8) X(8, 4) X(16, 4)
@@ -1031,11 +1074,16 @@ int leaf_set_smem(const FmmDev &f)
 {
     const int a = (int)p2p_smem(f), b = (int)l2p_smem(f);
     cudaError_t e = cudaSuccess;
-#define X(S_, B_)                                                                                  \
-    if (f.s == S_) {                                                                               \
-        if (a > 48 * 1024) e = cudaFuncSetAttribute(k_p2p<S_, B_>, cudaFuncAttributeMaxDynamicSharedMemorySize, a); \
-        if (e == cudaSuccess && b > 48 * 1024)                                                    \
-            e = cudaFuncSetAttribute(k_l2p<S_, B_>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); \
+#define X(S_, B_)                                                                                    \
+    if (f.s == S_ && a > 48 * 1024) {                                                                \
+        e = cudaFuncSetAttribute(k_p2p<S_, B_, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, a);   \
+        if (e == cudaSuccess)                                                                        \
+            e = cudaFuncSetAttribute(k_p2p<S_, B_, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, a); \
+    }                                                                                                \
+    if (f.s == S_ && e == cudaSuccess && b > 48 * 1024) {                                            \
+        e = cudaFuncSetAttribute(k_l2p<S_, B_, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);   \
+        if (e == cudaSuccess)                                                                        \
+            e = cudaFuncSetAttribute(k_l2p<S_, B_, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b); \
     }
     MMS_LEAF_CASES(X)
 #undef X
@@ -1049,7 +1097,14 @@ int leaf_set_smem(const FmmDev &f)
 int p2p_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float *Gn, float *out, cudaStream_t st)
 {
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
-#define X(S_, B_) if (f.s == S_) { MMS_CUDA_TRY(launch_k(k_p2p<S_, B_>, grid, dim3(leaf_threads(f)), p2p_smem(f), st, rho, Gn, out, f)); return MMS_OK; }
+#define X(S_, B_)                                                                                              \
+    if (f.s == S_) {                                                                                           \
+        if (p2p_groups(f) == 3)                                                                                \
+            MMS_CUDA_TRY(launch_k(k_p2p<S_, B_, 3>, grid, dim3(3 * leaf_threads(f)), p2p_smem(f), st, rho, Gn, out, f)); \
+        else                                                                                                   \
+            MMS_CUDA_TRY(launch_k(k_p2p<S_, B_, 1>, grid, dim3(leaf_threads(f)), p2p_smem(f), st, rho, Gn, out, f)); \
+        return MMS_OK;                                                                                         \
+    }
     MMS_LEAF_CASES(X)
 #undef X
     mms_set_error("no leaf kernel for side %d", f.s);
@@ -1061,7 +1116,16 @@ int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float
                const float *Lgp, const float *Lpp, cudaStream_t st)
 {
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
-#define X(S_, B_) if (f.s == S_) { MMS_CUDA_TRY(launch_k(k_l2p<S_, B_>, grid, dim3(leaf_threads(f)), l2p_smem(f), st, near, Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp)); return MMS_OK; }
+#define X(S_, B_)                                                                                              \
+    if (f.s == S_) {                                                                                           \
+        if (leaf_groups(f) == 3)                                                                               \
+            MMS_CUDA_TRY(launch_k(k_l2p<S_, B_, 3>, grid, dim3(3 * leaf_threads(f)), l2p_smem(f), st, near,      \
+                                  Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp));     \
+        else                                                                                                   \
+            MMS_CUDA_TRY(launch_k(k_l2p<S_, B_, 1>, grid, dim3(leaf_threads(f)), l2p_smem(f), st, near, Lpart_leaf, \
+                                  Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp));                \
+        return MMS_OK;                                                                                         \
+    }
     MMS_LEAF_CASES(X)
 #undef X
     mms_set_error("no leaf kernel for side %d", f.s);
