@@ -549,6 +549,49 @@ __device__ __forceinline__ void l2l_top_box(float *__restrict__ Lfin, const floa
     }
 }
 
+// The two top levels in one launch each way (NR <= 32).  CTA = one level-2
+// box.  Upward: its four level-3 children (one 4 KT-thread group each, from
+// their level-4 children), then the box itself from those four.  Downward:
+// the box's local from its M2L partials, then its four level-3 children.  The
+// same item code as the per-level kernels, so the same bits.
+__global__ void __launch_bounds__(512) k_top_m2m(float *__restrict__ Mall, const float *__restrict__ Tb,
+                                                 long long off2, long long off3, long long off4, FmmDev f)
+{
+    pdl_begin();
+    extern __shared__ __align__(16) float smb[];
+    const int NE = f.NE, NO = f.NR - f.NE;
+    const int tsz = 4 * (NE * NE + NO * NO);
+    const int KT = blockDim.x / 16;
+    float *Ts = smb;
+    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    __syncthreads();
+    const int grp = threadIdx.x / (4 * KT), t = threadIdx.x % (4 * KT);
+    float *Mc = Ts + tsz + grp * (4 * f.NR + 4 * KT), *red = Mc + 4 * f.NR;
+    const int P = blockIdx.x;
+    const int cx = 2 * (P % 4) + (grp & 1), cy = 2 * (P / 4) + (grp >> 1);
+    m2m_item(Mall, Ts, Mc, red, off3, off4, 8, cy * 8 + cx, f, t, KT, true);
+    m2m_item(Mall, Ts, Mc, red, off2, off3, 4, P, f, t, KT, grp == 0);
+}
+
+__global__ void __launch_bounds__(128) k_top_l2l(float *__restrict__ Lfin, const float *__restrict__ Lpart,
+                                                 const float *__restrict__ Tb, long long off2, long long off3,
+                                                 long long part_stride, int nsplit, FmmDev f)
+{
+    pdl_begin();
+    extern __shared__ __align__(16) float smb[];
+    const int NE = f.NE, NO = f.NR - f.NE;
+    const int tsz = 4 * (NE * NE + NO * NO);
+    const int KT = blockDim.x / 4;
+    float *Ts = smb, *Lp = smb + tsz;
+    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    const int P = blockIdx.x;
+    l2l_top_box(Lfin, Lpart, off2 + P, part_stride, nsplit, f, threadIdx.x, blockDim.x);
+    __syncthreads();
+    l2l_item(Lfin, Lpart, Ts, Lp, off2, off3, 8, 4, P, part_stride, nsplit, f, threadIdx.x, KT);
+}
+
 // Downward pass of one level: L(child) = sum of the NSPLIT M2L partials of the
 // child (fixed order) + L2L of the final parent local.  CTA per parent box,
 // thread per (child c, coefficient k); operator blocks and the parent local
@@ -1588,6 +1631,8 @@ size_t fmm_plan_bytes(const mms_ctx *ctx) { return ctx->fmm ? ctx->fmm->bytes : 
 // one 128-thread group per parent, 512 threads)
 static int l2p_up(const FmmPlan *pl) { return pl->d.L >= 3 && leaf_threads(pl->d) > 0 && !pl->far_fused; }
 static int p2m_up(const FmmPlan *pl) { return l2p_up(pl) && pl->d.NR <= 32; }
+// levels 2 and 3 share one launch each way (k_top_m2m / k_top_l2l: 16 KT <= 512 threads)
+static int top_two(const FmmPlan *pl) { return pl->d.NR <= 32 && !pl->far_fused; }
 
 // L2P of the far field onto the near field already in pl->near
 static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
@@ -1641,16 +1686,27 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         MMS_LAUNCH_CHECK(ctx);
         break;
     }
-    case 1:
-        // level L-1 is formed inside P2M when p2m_up()
-        for (int l = f.L - 1 - p2m_up(pl); l >= 2; l--) {
+    case 1: {
+        // level L-1 is formed inside P2M when p2m_up(); levels 3 and 2 in one
+        // launch when top_two()
+        const int lstart = f.L - 1 - p2m_up(pl);
+        const int top = top_two(pl) && lstart >= 3;
+        for (int l = lstart; l >= (top ? 4 : 2); l--) {
             const int np = 1 << l;
             MMS_CUDA_TRY(launch_k(k_m2m_c, dim3(np * np), dim3(4 * KT),
                                   (tsz + 4 * (size_t)f.NR + 4 * (size_t)KT) * sizeof(float), ctx->stream, pl->Mall,
                                   (const float *)pl->Tm2m, pl->lev_off[l], pl->lev_off[l + 1], np, f));
             MMS_LAUNCH_CHECK(ctx);
         }
+        if (top) {
+            MMS_CUDA_TRY(launch_k(k_top_m2m, dim3(16), dim3(16 * KT),
+                                  (tsz + 4 * (4 * (size_t)f.NR + 4 * (size_t)KT)) * sizeof(float), ctx->stream,
+                                  pl->Mall, (const float *)pl->Tm2m, pl->lev_off[2], pl->lev_off[3], pl->lev_off[4],
+                                  f));
+            MMS_LAUNCH_CHECK(ctx);
+        }
         break;
+    }
     case 2: {
         if (pl->m2l_tc) {
             k_m2l_gather<<<dim3(pl->tc_rows, 2), 256, 0, ctx->stream>>>(pl->Mall, pl->tcA[0], pl->tcA[1],
@@ -1683,13 +1739,19 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         // leaf level is formed inside the leaf kernel (or by k_l2l_c for the
         // generic leaf kernel)
         const int lend = leaf_threads(f) > 0 ? f.L - 1 - l2p_up(pl) : f.L;
-        if (lend >= 2) {
+        const int top = top_two(pl) && lend >= 3;
+        if (top) {
+            MMS_CUDA_TRY(launch_k(k_top_l2l, dim3(16), dim3(4 * KT), (tsz + (size_t)f.NR) * sizeof(float),
+                                  ctx->stream, pl->Lall, (const float *)pl->Lpart, (const float *)pl->Tl2l,
+                                  pl->lev_off[2], pl->lev_off[3], part_stride, nsplit, f));
+            MMS_LAUNCH_CHECK(ctx);
+        } else if (lend >= 2) {
             MMS_CUDA_TRY(launch_k(k_l2l_c, dim3(16), dim3(thr), 0, ctx->stream, pl->Lall,
                                   (const float *)pl->Lpart, (const float *)pl->Tl2l, 0LL, pl->lev_off[2], 4, 0,
                                   part_stride, nsplit, f));
             MMS_LAUNCH_CHECK(ctx);
         }
-        for (int l = 3; l <= lend; l++) {
+        for (int l = top ? 4 : 3; l <= lend; l++) {
             const int nc = 1 << l, np = nc / 2;
             MMS_CUDA_TRY(launch_k(k_l2l_c, dim3(np * np), dim3(4 * KT), (tsz + (size_t)f.NR) * sizeof(float),
                                   ctx->stream, pl->Lall, (const float *)pl->Lpart, (const float *)pl->Tl2l,
