@@ -530,6 +530,17 @@ def run_ensemble(args):
     if rank != 0:
         return 0
     value = args.steps / (ms_total * 1e-3)
+    # roofline of the batched exact potential, the dominant kernel: one FMA per
+    # (target, source) pair of every instance, 4 evaluations per RK4 step,
+    # over the whole step's time (a lower bound for the kernel's own rate)
+    pairs = float(sum((X * Y * Z) ** 2 for X, Y, Z in dims))
+    fma_peak = mmsb200.fma_tflops()
+    achieved = 4 * 2 * pairs / (ms_total / args.steps * 1e-3) / 1e12
+    roof = {"kernel": "k_ens_direct (batched exact potential)", "bound": "fp32", "unit": "TFLOP/s",
+            "achieved": achieved, "peak": fma_peak, "frac": achieved / fma_peak,
+            "peak_source": "measured FP32 FMA microbenchmark (mms_diag_fma_tflops), of measured",
+            "algorithmic": "2 flops per target-source pair, sum over instances of (cells)^2, 4 per step; "
+                           "timed over the whole step", "traffic": None}
     print(json.dumps({"metric": f"ensemble LLG RK4 steps/s ({args.ensemble_size} instances, 16..64 x 16..64 x 3)",
                       "value": value, "unit": "ensemble steps/s", "n_gpus": ws, "steps": args.steps,
                       "warmup": max(args.warmup, 3), "ms_per_step": ms_total / args.steps, "higher_is_better": True,
@@ -537,7 +548,8 @@ def run_ensemble(args):
                       "config": {"workload": "ensemble_rk4", "instances": args.ensemble_size, "cells": cells,
                                  "solver": "direct (batched)", "dt_s": args.dt,
                                  "l2": "flushed between timed steps", "parallelism": f"instance partition x{ws}"},
-                      "cell_steps_per_s": value * cells, "gpu_launches": int(launches), "clocks": clk}))
+                      "cell_steps_per_s": value * cells, "gpu_launches": int(launches), "clocks": clk,
+                      "roofline": roof}))
     return 0
 
 

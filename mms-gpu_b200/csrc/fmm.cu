@@ -504,8 +504,12 @@ __global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restr
     constexpr int NO_ = NR_ - NE_;
     constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
     extern __shared__ __align__(16) float sr[];
+    // stage the operator table with asynchronous copies: every 16-byte chunk
+    // in flight at once instead of one load-store round trip per chunk
     for (int i = threadIdx.x * 4; i < 49 * OSZ; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&sr[i]) = __ldg(reinterpret_cast<const float4 *>(&Tc[i]));
+        umma::cp_async16(umma::smem_u32(&sr[i]), &Tc[i], true);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     (void)f;
     m2l_res_item<NR_, NE_, true>(Mall, Lout, sr, sr, items[blockIdx.x], lev_off);
 }
