@@ -165,6 +165,17 @@ __global__ void k_l2p_p2p(const float *__restrict__ rho, const float *__restrict
 constexpr int BB = 8;         // leaf boxes per CTA along x in the leaf kernels
 constexpr int NSPLIT = 9;     // M2L offset groups (3 offsets each) -> partial locals
 
+// Stage n floats (n a multiple of 4, both addresses 16-byte aligned) into
+// shared memory with asynchronous copies, every chunk in flight at once, and
+// wait for this thread's copies; a __syncthreads must follow before any
+// other thread reads them.
+__device__ __forceinline__ void stage_async(float *dst, const float *src, int n)
+{
+    for (int i = threadIdx.x * 4; i < n; i += blockDim.x * 4) umma::cp_async16(umma::smem_u32(dst + i), src + i, true);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // P2M of one item = BB leaf boxes of one row: the boxes' charges are staged
 // transposed in shared memory ([cell][box]); thread per (box, coefficient),
 // each output summed over the cells in order.  Wt: [C][NR] weights (shared or
@@ -212,8 +223,7 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
     if (wsm) {
         float *Ws = tail;
         const int n = f.C * f.NR;
-        for (int i = threadIdx.x * 4; i < n; i += blockDim.x * 4)
-            *reinterpret_cast<float4 *>(&Ws[i]) = __ldg(reinterpret_cast<const float4 *>(&Wg[i]));
+        stage_async(Ws, Wg, n);
         Wt = Ws;
         tail += n;
     }
@@ -227,8 +237,7 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
     const int tsz = 4 * (NE * NE + NO * NO);
     const int KT = ((f.NR + 31) / 32) * 32;
     float *Ts = tail, *scr = Ts + tsz;
-    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tm2m[i]));
+    stage_async(Ts, Tm2m, tsz);
     for (int i = threadIdx.x; i < 2 * CB; i += blockDim.x) {
         const int r = i / CB, j = i % CB, b = j % BB, c = j / BB;
         const int x = (bx0 + b) * s + c % s, y = (2 * blockIdx.y + r) * s + (c / s) % s, z = c / (s * s);
@@ -302,8 +311,7 @@ __global__ void k_m2m_c(float *__restrict__ Mall, const float *__restrict__ Tb, 
     float *Ts = smb;                          // [4][blocks]
     float *Mc = smb + tsz;                    // [4][NR]
     float *red = Mc + 4 * f.NR;               // [4][KT]
-    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    stage_async(Ts, Tb, tsz);
     m2m_item(Mall, Ts, Mc, red, off_p, off_c, np, blockIdx.x, f, threadIdx.x, KT);
 }
 
@@ -356,8 +364,7 @@ __global__ void __launch_bounds__(32 * M2L_WARPS) k_m2l_split(const float *__res
             const int o = (oy + 3) * 7 + (ox + 3);
             const float *Tg = Tm2l + ((long long)o * 2 + blk) * NBmax * KPmax;
             __syncthreads();
-            for (int i = threadIdx.x * 4; i < NB * KP; i += blockDim.x * 4)
-                *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tg[i]));
+            stage_async(Ts, Tg, NB * KP);
             for (int i = threadIdx.x; i < 32 * NB; i += blockDim.x) {
                 const int t = i / NB, j = i % NB;
                 const int tj = it.z + t;
@@ -567,8 +574,7 @@ __global__ void __launch_bounds__(512) k_top_m2m(float *__restrict__ Mall, const
     const int tsz = 4 * (NE * NE + NO * NO);
     const int KT = blockDim.x / 16;
     float *Ts = smb;
-    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    stage_async(Ts, Tb, tsz);
     __syncthreads();
     const int grp = threadIdx.x / (4 * KT), t = threadIdx.x % (4 * KT);
     float *Mc = Ts + tsz + grp * (4 * f.NR + 4 * KT), *red = Mc + 4 * f.NR;
@@ -588,8 +594,7 @@ __global__ void __launch_bounds__(128) k_top_l2l(float *__restrict__ Lfin, const
     const int tsz = 4 * (NE * NE + NO * NO);
     const int KT = blockDim.x / 4;
     float *Ts = smb, *Lp = smb + tsz;
-    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    stage_async(Ts, Tb, tsz);
     const int P = blockIdx.x;
     l2l_top_box(Lfin, Lpart, off2 + P, part_stride, nsplit, f, threadIdx.x, blockDim.x);
     __syncthreads();
@@ -614,8 +619,7 @@ __global__ void k_l2l_c(float *__restrict__ Lfin, const float *__restrict__ Lpar
     const int KT = blockDim.x / 4;
     float *Ts = smb;          // [4][blocks]
     float *Lp = smb + tsz;    // [NR]
-    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
-        *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tb[i]));
+    stage_async(Ts, Tb, tsz);
     l2l_item(Lfin, Lpart, Ts, Lp, off_p, off_c, nc, np, blockIdx.x, part_stride, nsplit, f, threadIdx.x, KT);
 }
 
@@ -715,6 +719,7 @@ __global__ void __launch_bounds__(32 * RES_WARPS) k_far(const float *__restrict_
     for (int i = tid * 4; i < 49 * OSZ; i += blockDim.x * 4)
         umma::cp_async16(umma::smem_u32(Tl + i), Tm2lc + i, true);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // synchronous: the M2L table's asynchronous copies stay in flight meanwhile
     for (int i = tid * 4; i < 4 * OSZ; i += blockDim.x * 4) {
         *reinterpret_cast<float4 *>(&Tu[i]) = __ldg(reinterpret_cast<const float4 *>(&Tm2m[i]));
         *reinterpret_cast<float4 *>(&Td[i]) = __ldg(reinterpret_cast<const float4 *>(&Tl2l[i]));
@@ -879,8 +884,7 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
     const int np = f.nb >> 1, prow = by >> 1;
     if (haspar) {
         const int tsz = 4 * (NE * NE + NO * NO);
-        for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
-            *reinterpret_cast<float4 *>(&Ts[i]) = __ldg(reinterpret_cast<const float4 *>(&Tl2l[i]));
+        stage_async(Ts, Tl2l, tsz);
     }
     if (pmode == 1) {
         for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
