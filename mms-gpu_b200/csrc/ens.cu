@@ -10,7 +10,8 @@
 // (instance, block of target rows) items: several short target rows share a
 // warp, each lane keeps 8 consecutive targets in registers and slides a window
 // over a mirrored table G[|dz|][|dy|][.] = dV/|r| kept in shared memory, with
-// the source row broadcast from shared memory (one FMA per pair).
+// the source row broadcast from shared memory (one FMA per pair); FP32 sums
+// over groups of KG source rows are combined with Kahan compensation.
 //
 // Per-step physics is the single-grid path's (stencil_dev.cuh); each instance
 // has its own constant external field.
@@ -28,9 +29,10 @@ namespace {
 using namespace mmsdev;
 
 constexpr int ETPB = 256;       // cells per tile / threads per block in the cell kernels
-constexpr int EW = 4;           // warps per CTA in the batched direct kernel
+constexpr int EW = 8;           // warps per CTA in the batched direct kernel
 constexpr int ETX = 8;          // targets per lane
-constexpr int QROWS = 8;        // source rows staged per batch
+constexpr int QROWS = 16;       // source rows staged per batch
+constexpr int KG = 4;           // source rows summed in FP32 between compensated (Kahan) adds
 
 struct EnsInst {
     int X, Y, Z;
@@ -216,23 +218,34 @@ __global__ void __launch_bounds__(EW * 32) k_ens_direct(const float *__restrict_
         }
         __syncthreads();
         if (!active) continue;
+        float acc[ETX];
+#pragma unroll
+        for (int i = 0; i < ETX; i++) acc[i] = 0.f;
         for (int qr = 0; qr < nq; qr++) {
             const int srow = sr0 + qr;
             const int ys = srow % in.Y, zs = srow / in.Y;
             const float *grow = gm + (abs(zt - zs) * t.Ym + abs(yt - ys)) * t.pitch;
             const float *q = qs + qr * t.Xm;
-            float acc[ETX];
-#pragma unroll
-            for (int i = 0; i < ETX; i++) acc[i] = 0.f;
             // window: win[k] = grow[base + k], base = C - 7 + x0 - xb
+            // C = Xm + 3 with Xm a multiple of 8: base is a multiple of 4, so
+            // the window is read as two 16-byte vectors (a row's lanes are 32 B
+            // apart: at most 2-way bank conflicts instead of 8-way scalar ones)
             int base = t.C - 7 + x0;
             float wb[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) wb[k] = grow[base + 8 + k];
+            {
+                const float4 u0 = *reinterpret_cast<const float4 *>(grow + base + 8);
+                const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 12);
+                wb[0] = u0.x; wb[1] = u0.y; wb[2] = u0.z; wb[3] = u0.w;
+                wb[4] = u1.x; wb[5] = u1.y; wb[6] = u1.z; wb[7] = u1.w;
+            }
             for (int xb = 0; xb < Xr; xb += 8) {
                 float wa[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++) wa[k] = grow[base + k];
+                {
+                    const float4 u0 = *reinterpret_cast<const float4 *>(grow + base);
+                    const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 4);
+                    wa[0] = u0.x; wa[1] = u0.y; wa[2] = u0.z; wa[3] = u0.w;
+                    wa[4] = u1.x; wa[5] = u1.y; wa[6] = u1.z; wa[7] = u1.w;
+                }
                 const float4 q0 = *reinterpret_cast<const float4 *>(&q[xb]);
                 const float4 q1 = *reinterpret_cast<const float4 *>(&q[xb + 4]);
                 const float qv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
@@ -247,12 +260,15 @@ __global__ void __launch_bounds__(EW * 32) k_ens_direct(const float *__restrict_
                 for (int k = 0; k < 8; k++) wb[k] = wa[k];
                 base -= 8;
             }
+            if ((qr + 1) % KG == 0 || qr + 1 == nq) {
 #pragma unroll
-            for (int i = 0; i < ETX; i++) {  // Kahan across source rows
-                const float y = acc[i] - c[i];
-                const float tt = s[i] + y;
-                c[i] = (tt - s[i]) - y;
-                s[i] = tt;
+                for (int i = 0; i < ETX; i++) {  // Kahan across groups of KG source rows
+                    const float y = acc[i] - c[i];
+                    const float tt = s[i] + y;
+                    c[i] = (tt - s[i]) - y;
+                    s[i] = tt;
+                    acc[i] = 0.f;
+                }
             }
         }
     }
