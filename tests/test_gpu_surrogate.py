@@ -195,3 +195,24 @@ def test_trained_network_gain_over_near_field_only(cuda, lib):
     assert e_sur < 0.1 * e_near    # the network recovers > 90 % of it
     assert e_sur < 0.05
     assert e_fmm < 1e-3            # the check's reference is within the target
+
+
+@pytest.mark.parametrize("tol,stays", [(1e9, True), (1e-9, False)])
+def test_march_checks_on_rejected_steps(cuda, lib, tol, stays):
+    """mms_march (step doubling) checks the surrogate on every rejected step:
+    an oversized first step is rejected, the check runs, and with a tight
+    tolerance the FMM takes over for the rest of the march, which still ends
+    at the final time"""
+    import mmsb200
+    from mmsb200 import geometry, surrogate
+    w, _ = surrogate.load_weights()
+    assert w is not None
+    mask = geometry.disc(48, 48, 3, 22)
+    M = geometry.random_inplane(mask, 21)
+    with _surrogate_ctx(mmsb200, mask, M, w, 100000, tol) as ctx:
+        rows, st = ctx.march(2e-12, 1e-11, mode=1, rtol=1e-6, torque_stop=0.0)
+        _, t = ctx.state_get()
+        s = ctx.surrogate_stats()
+    assert st == mmsb200.MMS_OK and abs(t - 2e-12) < 1e-24
+    assert s["checks"] >= 1
+    assert s["active"] == stays and s["fallbacks"] == (0 if stays else 1)
