@@ -209,12 +209,17 @@ __global__ void __launch_bounds__(EW * 32) k_ens_direct(const float *__restrict_
     float s[ETX], c[ETX];
 #pragma unroll
     for (int i = 0; i < ETX; i++) s[i] = c[i] = 0.f;
+    __shared__ int nz[QROWS];  // staged source row holds a non-zero charge
     for (int sr0 = 0; sr0 < nrows; sr0 += QROWS) {
+        __syncthreads();
+        if (threadIdx.x < QROWS) nz[threadIdx.x] = 0;
         __syncthreads();
         const int nq = min(QROWS, nrows - sr0);
         for (int i = threadIdx.x; i < QROWS * t.Xm; i += blockDim.x) {
             const int qr = i / t.Xm, xs = i % t.Xm;
-            qs[i] = (qr < nq && xs < in.X) ? rho[in.off + (long long)(sr0 + qr) * in.X + xs] : 0.f;
+            const float v = (qr < nq && xs < in.X) ? rho[in.off + (long long)(sr0 + qr) * in.X + xs] : 0.f;
+            qs[i] = v;
+            if (v != 0.f) nz[qr] = 1;  // benign race: every writer stores 1
         }
         __syncthreads();
         if (!active) continue;
@@ -222,43 +227,45 @@ __global__ void __launch_bounds__(EW * 32) k_ens_direct(const float *__restrict_
 #pragma unroll
         for (int i = 0; i < ETX; i++) acc[i] = 0.f;
         for (int qr = 0; qr < nq; qr++) {
-            const int srow = sr0 + qr;
-            const int ys = srow % in.Y, zs = srow / in.Y;
-            const float *grow = gm + (abs(zt - zs) * t.Ym + abs(yt - ys)) * t.pitch;
-            const float *q = qs + qr * t.Xm;
-            // window: win[k] = grow[base + k], base = C - 7 + x0 - xb
-            // C = Xm + 3 with Xm a multiple of 8: base is a multiple of 4, so
-            // the window is read as two 16-byte vectors (a row's lanes are 32 B
-            // apart: at most 2-way bank conflicts instead of 8-way scalar ones)
-            int base = t.C - 7 + x0;
-            float wb[8];
-            {
-                const float4 u0 = *reinterpret_cast<const float4 *>(grow + base + 8);
-                const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 12);
-                wb[0] = u0.x; wb[1] = u0.y; wb[2] = u0.z; wb[3] = u0.w;
-                wb[4] = u1.x; wb[5] = u1.y; wb[6] = u1.z; wb[7] = u1.w;
-            }
-            for (int xb = 0; xb < Xr; xb += 8) {
-                float wa[8];
+            if (nz[qr]) {  // an all-zero source row adds nothing
+                const int srow = sr0 + qr;
+                const int ys = srow % in.Y, zs = srow / in.Y;
+                const float *grow = gm + (abs(zt - zs) * t.Ym + abs(yt - ys)) * t.pitch;
+                const float *q = qs + qr * t.Xm;
+                // window: win[k] = grow[base + k], base = C - 7 + x0 - xb
+                // C = Xm + 3 with Xm a multiple of 8: base is a multiple of 4, so
+                // the window is read as two 16-byte vectors (a row's lanes are 32 B
+                // apart: at most 2-way bank conflicts instead of 8-way scalar ones)
+                int base = t.C - 7 + x0;
+                float wb[8];
                 {
-                    const float4 u0 = *reinterpret_cast<const float4 *>(grow + base);
-                    const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 4);
-                    wa[0] = u0.x; wa[1] = u0.y; wa[2] = u0.z; wa[3] = u0.w;
-                    wa[4] = u1.x; wa[5] = u1.y; wa[6] = u1.z; wa[7] = u1.w;
+                    const float4 u0 = *reinterpret_cast<const float4 *>(grow + base + 8);
+                    const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 12);
+                    wb[0] = u0.x; wb[1] = u0.y; wb[2] = u0.z; wb[3] = u0.w;
+                    wb[4] = u1.x; wb[5] = u1.y; wb[6] = u1.z; wb[7] = u1.w;
                 }
-                const float4 q0 = *reinterpret_cast<const float4 *>(&q[xb]);
-                const float4 q1 = *reinterpret_cast<const float4 *>(&q[xb + 4]);
-                const float qv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-#pragma unroll
-                for (int j = 0; j < 8; j++)
-#pragma unroll
-                    for (int i = 0; i < ETX; i++) {
-                        const int k = 7 + i - j;
-                        acc[i] = fmaf(qv[j], (k < 8) ? wa[k] : wb[k - 8], acc[i]);
+                for (int xb = 0; xb < Xr; xb += 8) {
+                    float wa[8];
+                    {
+                        const float4 u0 = *reinterpret_cast<const float4 *>(grow + base);
+                        const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 4);
+                        wa[0] = u0.x; wa[1] = u0.y; wa[2] = u0.z; wa[3] = u0.w;
+                        wa[4] = u1.x; wa[5] = u1.y; wa[6] = u1.z; wa[7] = u1.w;
                     }
-#pragma unroll
-                for (int k = 0; k < 8; k++) wb[k] = wa[k];
-                base -= 8;
+                    const float4 q0 = *reinterpret_cast<const float4 *>(&q[xb]);
+                    const float4 q1 = *reinterpret_cast<const float4 *>(&q[xb + 4]);
+                    const float qv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    #pragma unroll
+                    for (int j = 0; j < 8; j++)
+    #pragma unroll
+                        for (int i = 0; i < ETX; i++) {
+                            const int k = 7 + i - j;
+                            acc[i] = fmaf(qv[j], (k < 8) ? wa[k] : wb[k - 8], acc[i]);
+                        }
+    #pragma unroll
+                    for (int k = 0; k < 8; k++) wb[k] = wa[k];
+                    base -= 8;
+                }
             }
             if ((qr + 1) % KG == 0 || qr + 1 == nq) {
 #pragma unroll
