@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(DWARPS * 32) k_direct(const float *__restrict_
         const float *rba = rho + (long long)zb * plane + (long long)ya * g.X;
         const float *rbb = rho + (long long)zb * plane + (long long)yb * g.X;
         __syncwarp();
+        bool nzl = false;
         for (int k = lane; k < sh.Xr; k += 32) {
             float q = 0.f;
             if (k < g.X) {
@@ -107,7 +108,11 @@ __global__ void __launch_bounds__(DWARPS * 32) k_direct(const float *__restrict_
                 if (hzb && hyb) q += rbb[k];
             }
             qs[k] = q;
+            nzl |= q != 0.f;
         }
+        // a group whose source rows carry no charge adds nothing: skip it
+        // (e.g. the empty padding layers of an in-plane magnetised film)
+        if (!__any_sync(0xffffffffu, nzl)) continue;
         const float *grow = gtab + ((long long)adz * g.Y + ady) * g.X;
         for (int k = lane; k < sh.GM; k += 32) {
             const int d = abs(k - sh.C);
