@@ -785,11 +785,16 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
     constexpr int W = (BB + 2) * S;        // charges per staged row
     float *qn = sl;                        // [Z][3S][W]
     float *g = qn + Z * 3 * S * W;         // [Z][2S][2S]
+    __shared__ int nzr[384];               // staged source row (z, y) holds charge; Z 3S <= 384 whenever BB S Z <= 512
     const int by = blockIdx.y, bx0 = blockIdx.x * BB;
     const int xs0 = bx0 * S - S, ys0 = by * S - S;
+    for (int i = threadIdx.x; i < Z * 3 * S; i += blockDim.x) nzr[i] = 0;
+    __syncthreads();
     for (int i = threadIdx.x; i < Z * 3 * S * W; i += blockDim.x) {
         const int xx = xs0 + i % W, yy = ys0 + (i / W) % (3 * S), zz = i / (W * 3 * S);
-        qn[i] = (xx >= 0 && yy >= 0 && xx < f.X && yy < f.Y) ? rho[((long long)zz * f.Y + yy) * f.X + xx] : 0.f;
+        const float v = (xx >= 0 && yy >= 0 && xx < f.X && yy < f.Y) ? rho[((long long)zz * f.Y + yy) * f.X + xx] : 0.f;
+        qn[i] = v;
+        if (v != 0.f) nzr[i / W] = 1;  // benign race: every writer stores 1
     }
     for (int i = threadIdx.x; i < Z * 4 * S * S; i += blockDim.x) g[i] = Gn[i];
     __syncthreads();
@@ -804,6 +809,7 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
     for (int zs = 0; zs < Z; zs++) {
         const int dz = abs(zs - lz);
         for (int ys = grp * RG; ys < (grp + 1) * RG; ys++) {
+            if (!nzr[zs * 3 * S + ys]) continue;  // no charge in this source row (uniform per warp)
             const int dy = abs(ys - ly - S);
             const float *grow = g + (dz * 2 * S + dy) * 2 * S;
             const float *qrow = qn + (zs * 3 * S + ys) * W + b * S;
