@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--solver", choices=["fmm", "direct"], default=os.environ.get("MMS_BENCH_SOLVER", "fmm"))
     ap.add_argument("--order", type=int, default=4,
                     help="FMM expansion order P; 0 = autotuned on RK4 steps (fastest within 5e-4 of the exact sum)")
-    ap.add_argument("--leaf", type=int, default=4, help="FMM leaf side in cells (0 = the library's default)")
+    ap.add_argument("--leaf", type=int, default=8, help="FMM leaf side in cells (0 = the library's default)")
     ap.add_argument("--m2l", type=int, default=int(os.environ.get("MMS_BENCH_M2L", "0")),
                     help="FMM M2L: 0 auto, 1 FP32 SIMT, 2 tensor cores (split BF16)")
     ap.add_argument("--size", type=int, default=256)

@@ -95,7 +95,9 @@ struct FmmPlan {
     float *Mall = nullptr;    // [boxes of all levels][NR]
     float *Lall = nullptr;    // final locals
     float *Lpart = nullptr;   // [NSPLIT][boxes][NR] M2L partial locals
-    int4 *m2l_items = nullptr;  // {level, parity, first target, 0}
+    int4 *m2l_items = nullptr;  // {level, parity, first target, 0}: 32 targets (k_m2l_split)
+    int4 *res_items = nullptr;  // the same with RES_TPI targets (k_m2l_res, k_far)
+    int n_res_items = 0;
     long long *lev_dev = nullptr;  // device copy of lev_off
     float *near = nullptr;    // [N] near-field potential (P2P) before L2P adds the far field
     cudaStream_t side = nullptr;   // P2P runs here, concurrently with P2M .. L2L
@@ -405,32 +407,42 @@ __global__ void __launch_bounds__(32 * M2L_WARPS) k_m2l_split(const float *__res
 // partials are summed in a fixed order in shared memory; the result is the
 // complete M2L local (one partial buffer).
 constexpr int RES_WARPS = 8;
+constexpr int RES_TPI = 16;  // targets per resident-M2L item
 
 // one M2L item (32 targets of one level and parity class, all 27 offsets) on
 // RES_WARPS warps; Ts = all 49 operator slots in shared memory; red =
 // RES_WARPS * 32 * (NR + 1) floats of shared scratch (may alias Ts: it is
 // written only after the last operator read)
+// one M2L item (RES_TPI = 16 targets of one level and parity class, all 27
+// offsets) on RES_WARPS warps; lane = (half, target): the 16 slots (warp,
+// half) take the class's offsets s, s + 16 (class order), the two halves of a
+// warp are added with one shuffle and the warps in a fixed order.  Ts = all
+// 49 operator slots in shared memory; red = RES_WARPS * RES_TPI * (NR + 1)
+// floats of shared scratch (may alias Ts: it is written only after the last
+// operator read)
 template <int NR_, int NE_, bool NC>
 __device__ __forceinline__ void m2l_res_item(const float *__restrict__ Mall, float *__restrict__ Lout, const float *Ts,
                                              float *red, const int4 it, const long long *__restrict__ lev_off)
 {
     constexpr int NO_ = NR_ - NE_;
     constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
+    constexpr int NSLOT = 2 * RES_WARPS;
     const int lev = it.x, px = it.y & 1, py = it.y >> 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int half = lane >> 4, tl = lane & 15, slot = 2 * warp + half;
     const int n = 1 << lev, nh = n >> 1;
     const long long off = lev_off[lev];
-    const int ti = it.z + lane;
+    const int ti = it.z + tl;
     const bool tvalid = ti < nh * nh;
     const int tx = 2 * (ti % nh) + px, ty = 2 * (ti / nh) + py;
-    // this warp's offsets (w, w+8, ...) of the class's 27, in class order
-    int ox_l[4], oy_l[4], no = 0;
+    // this slot's offsets (s, s + 16) of the class's 27, in class order
+    int ox_l[2], oy_l[2], no = 0;
     {
         int idx = 0;
         for (int oy = py - 3; oy <= py + 2; oy++)
             for (int ox = px - 3; ox <= px + 2; ox++) {
                 if (max(abs(ox), abs(oy)) < 2) continue;
-                if ((idx++ % RES_WARPS) == warp && no < 4) {
+                if ((idx++ % NSLOT) == slot && no < 2) {
                     ox_l[no] = ox;
                     oy_l[no] = oy;
                     no++;
@@ -455,7 +467,7 @@ __device__ __forceinline__ void m2l_res_item(const float *__restrict__ Mall, flo
     if (no > 0) fetch(0, m);
     __syncthreads();
 #pragma unroll 1
-    for (int q = 0; q < 4; q++) {
+    for (int q = 0; q < 2; q++) {
         if (q >= no) break;
         if (q + 1 < no) fetch(q + 1, mn);
         const float *T = Ts + ((oy_l[q] + 3) * 7 + (ox_l[q] + 3)) * OSZ;
@@ -483,19 +495,24 @@ __device__ __forceinline__ void m2l_res_item(const float *__restrict__ Mall, flo
 #pragma unroll
         for (int k = 0; k < NR_; k++) m[k] = mn[k];
     }
-    __syncthreads();  // (when red aliases Ts) operators no longer needed
-    float *rw = red + (warp * 32 + lane) * (NR_ + 1);
+    // the two halves of the warp hold the same targets: lower + upper
 #pragma unroll
-    for (int k = 0; k < NR_; k++) rw[k] = acc[k];
+    for (int k = 0; k < NR_; k++) acc[k] += __shfl_down_sync(0xffffffffu, acc[k], 16);
+    __syncthreads();  // (when red aliases Ts) operators no longer needed
+    if (half == 0) {
+        float *rw = red + (warp * RES_TPI + tl) * (NR_ + 1);
+#pragma unroll
+        for (int k = 0; k < NR_; k++) rw[k] = acc[k];
+    }
     __syncthreads();
     // fixed-order sum over the warps: thread t handles (target, k) pairs
-    for (int e = threadIdx.x; e < 32 * NR_; e += blockDim.x) {
+    for (int e = threadIdx.x; e < RES_TPI * NR_; e += blockDim.x) {
         const int t = e / NR_, k = e % NR_;
         const int tj = it.z + t;
         if (tj >= nh * nh) continue;
         float v = 0.f;
 #pragma unroll
-        for (int w = 0; w < RES_WARPS; w++) v += red[(w * 32 + t) * (NR_ + 1) + k];
+        for (int w = 0; w < RES_WARPS; w++) v += red[(w * RES_TPI + t) * (NR_ + 1) + k];
         const int ux = 2 * (tj % nh) + px, uy = 2 * (tj / nh) + py;
         Lout[(off + (long long)uy * n + ux) * NR_ + k] = v;
     }
@@ -692,7 +709,7 @@ constexpr int far_scratch(int C)
 {
     constexpr int KT = far_kt<NR_>();
     constexpr int G = (32 * RES_WARPS) / (4 * KT);
-    const int a = C * BB, b = RES_WARPS * 32 * (NR_ + 1), c = G * (4 * NR_ + 4 * KT + NR_);
+    const int a = C * BB, b = RES_WARPS * RES_TPI * (NR_ + 1), c = G * (4 * NR_ + 4 * KT + NR_);
     return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
 
@@ -1203,7 +1220,7 @@ int m2l_res_supported(int NR, int NE)
 size_t m2l_res_smem(int NR, int NE)
 {
     const int NO = NR - NE;
-    return std::max((size_t)49 * (NE * NE + NO * NO), (size_t)RES_WARPS * 32 * (NR + 1)) * sizeof(float);
+    return std::max((size_t)49 * (NE * NE + NO * NO), (size_t)RES_WARPS * RES_TPI * (NR + 1)) * sizeof(float);
 }
 
 int m2l_res_prepare(int NR, int NE)
@@ -1419,6 +1436,13 @@ int fmm_plan_create(mms_ctx *ctx)
             for (int t0 = 0; t0 < nh * nh; t0 += 32) items.push_back(make_int4(l, par, t0, 0));
     }
     pl->n_m2l_items = (int)items.size();
+    std::vector<int4> ritems;
+    for (int l = 2; l <= f.L; l++) {
+        const int nh = (1 << l) / 2;
+        for (int par = 0; par < 4; par++)
+            for (int t0 = 0; t0 < nh * nh; t0 += RES_TPI) ritems.push_back(make_int4(l, par, t0, 0));
+    }
+    pl->n_res_items = (int)ritems.size();
 
     // tensor-core M2L rows: every box of levels >= 2, grouped by parity class
     std::vector<int> tc_rowmap;
@@ -1483,6 +1507,7 @@ int fmm_plan_create(mms_ctx *ctx)
         }
     }
     if (!st) st = upload(ctx, pl, &pl->m2l_items, items);
+    if (!st) st = upload(ctx, pl, &pl->res_items, ritems);
     long long *lev_dev = nullptr;
     if (!st) st = upload(ctx, pl, &lev_dev, pl->lev_off);
     if (st) {
@@ -1625,7 +1650,7 @@ void fmm_plan_destroy(mms_ctx *ctx)
     if (!pl) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Tm2lc, pl->Gn, pl->Mall, pl->Lall, pl->Lpart,
-                 pl->m2l_items, pl->lev_dev, pl->near, pl->tcA[0], pl->tcA[1], pl->tcB, pl->tc_rowmap,
+                 pl->m2l_items, pl->res_items, pl->lev_dev, pl->near, pl->tcA[0], pl->tcA[1], pl->tcB, pl->tc_rowmap,
                  pl->tc_rowinfo, pl->tc_groups, pl->far_sync};
     for (void *p : b)
         if (p) cudaFree(p);
@@ -1734,7 +1759,7 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
             break;
         }
         if (pl->m2l_resident) {
-            MMS_TRY(m2l_res_launch(f, pl->n_m2l_items, pl->Mall, pl->Lpart, pl->Tm2lc, pl->m2l_items, pl->lev_dev,
+            MMS_TRY(m2l_res_launch(f, pl->n_res_items, pl->Mall, pl->Lpart, pl->Tm2lc, pl->res_items, pl->lev_dev,
                                    ctx->stream));
         } else {
             const int NBmax = std::max(f.NE, f.NR - f.NE);
@@ -1855,7 +1880,7 @@ int far_launch(mms_ctx *ctx, const float *rho)
     if (f.NR == a && f.NE == c) {                                                                                 \
         MMS_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_far<a, c>, rho, (const float *)pl->Wt, pl->Mall, pl->Lpart,        \
                                         pl->Lall, (const float *)pl->Tm2m, (const float *)pl->Tm2lc,                \
-                                        (const float *)pl->Tl2l, (const int4 *)pl->m2l_items, pl->n_m2l_items,      \
+                                        (const float *)pl->Tl2l, (const int4 *)pl->res_items, pl->n_res_items,      \
                                         (const long long *)pl->lev_dev, f, nbx, nby, lend, pl->far_sync));         \
         MMS_LAUNCH_CHECK(ctx);                                                                                    \
         return MMS_OK;                                                                                            \
