@@ -1119,10 +1119,10 @@ int leaf_threads(const FmmDev &f)
 // thread groups per leaf box in k_l2p (on the critical path after the join):
 // 3 while the CTA stays <= 512 threads
 int leaf_groups(const FmmDev &f) { return 3 * leaf_threads(f) <= 512 ? 3 : 1; }
-// in k_p2p, which runs beside the far-field chain: wider CTAs pay off while the
-// near field is small (leaf <= 4); at leaf 8 they crowd the far chain's kernels
-// off the SMs (measured: 3530 -> 3262 steps/s at 256 x 256 x 3)
-int p2p_groups(const FmmDev &f) { return f.s <= 4 ? leaf_groups(f) : 1; }
+// in k_p2p, which runs beside the far-field chain: the same three groups (once
+// the far chain was shortened, the near field became the longer branch at
+// leaf 8 and the wider CTAs paid off there too: 3980 -> 4126 steps/s)
+int p2p_groups(const FmmDev &f) { return leaf_groups(f); }
 
 size_t p2p_smem(const FmmDev &f)
 {
