@@ -207,12 +207,14 @@ __device__ __forceinline__ void m2m_item(float *__restrict__ Mall, const float *
                                          int KT, bool valid);
 
 // P2M: CTA = one item (BB leaf boxes of one row).  With up != 0 (NR <= 32)
-// the CTA takes two leaf rows (both in parallel, thread per (row, box,
-// coefficient)) and then forms their BB/2 parents (the M2M of level L-1) with
-// one 4 KT-thread group per parent, reading the children it just wrote; 512
-// threads.  Per output the same summation order as p2m_item / m2m_item.
+// the CTA takes PB boxes of two leaf rows (both in parallel, thread per (row,
+// box, coefficient)) and then forms their PB/2 parents (the M2M of level L-1)
+// with one 4 KT-thread group per parent, reading the children it just wrote;
+// PB/2 x 128 threads.  PB = 8, or 4 at leaf side >= 8 (twice the CTAs where
+// the boxes are large and few).  Per output the same summation order as p2m_item / m2m_item.
 // Shared memory: charges [rows][C][BB], W [C][NR] when wsm, then (up) the M2M
 // operators and the per-parent M2M scratch.
+template <int PB>
 __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, const float *__restrict__ Wg,
                                                  float *__restrict__ Mall, long long off_leaf, FmmDev f, int wsm,
                                                  int up, const float *__restrict__ Tm2m, long long off_par)
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
     extern __shared__ __align__(16) float q[];
     const int rows = up ? 2 : 1;
     const float *Wt = Wg;
-    float *tail = q + rows * f.C * BB;
+    float *tail = q + rows * f.C * PB;
     if (wsm) {
         float *Ws = tail;
         const int n = f.C * f.NR;
@@ -230,28 +232,28 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
         tail += n;
     }
     float *Mleaf = Mall + off_leaf * f.NR;
-    const int bx0 = blockIdx.x * BB;
+    const int bx0 = blockIdx.x * PB;
     if (!up) {
-        p2m_item(rho, Wt, q, Mleaf, f, blockIdx.y, bx0);
+        if constexpr (PB == BB) p2m_item(rho, Wt, q, Mleaf, f, blockIdx.y, bx0);
         return;
     }
-    const int NE = f.NE, NO = f.NR - f.NE, s = f.s, CB = f.C * BB;
+    const int NE = f.NE, NO = f.NR - f.NE, s = f.s, CB = f.C * PB;
     const int tsz = 4 * (NE * NE + NO * NO);
     const int KT = ((f.NR + 31) / 32) * 32;
     float *Ts = tail, *scr = Ts + tsz;
     stage_async(Ts, Tm2m, tsz);
     for (int i = threadIdx.x; i < 2 * CB; i += blockDim.x) {
-        const int r = i / CB, j = i % CB, b = j % BB, c = j / BB;
+        const int r = i / CB, j = i % CB, b = j % PB, c = j / PB;
         const int x = (bx0 + b) * s + c % s, y = (2 * blockIdx.y + r) * s + (c / s) % s, z = c / (s * s);
         q[i] = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < 2 * BB * f.NR; e += blockDim.x) {
-        const int r = e / (BB * f.NR), rem = e % (BB * f.NR), b = rem / f.NR, k = rem % f.NR;
+    for (int e = threadIdx.x; e < 2 * PB * f.NR; e += blockDim.x) {
+        const int r = e / (PB * f.NR), rem = e % (PB * f.NR), b = rem / f.NR, k = rem % f.NR;
         const float *qr = q + r * CB;
         float acc = 0.f;
 #pragma unroll 4
-        for (int c = 0; c < f.C; c++) acc = fmaf(Wt[(long long)c * f.NR + k], qr[c * BB + b], acc);
+        for (int c = 0; c < f.C; c++) acc = fmaf(Wt[(long long)c * f.NR + k], qr[c * PB + b], acc);
         if (bx0 + b < f.nb) Mleaf[((long long)(2 * blockIdx.y + r) * f.nb + bx0 + b) * f.NR + k] = acc;
     }
     __syncthreads();
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
     const int grp = threadIdx.x / (4 * KT), t = threadIdx.x % (4 * KT);
     const int pc = (bx0 >> 1) + grp;
     float *Mc = scr + grp * (4 * f.NR + 4 * KT), *red = Mc + 4 * f.NR;
-    m2m_item(Mall, Ts, Mc, red, off_par, off_leaf, np, blockIdx.y * np + pc, f, t, KT, grp < BB / 2 && pc < np);
+    m2m_item(Mall, Ts, Mc, red, off_par, off_leaf, np, blockIdx.y * np + pc, f, t, KT, grp < PB / 2 && pc < np);
 }
 
 // M2M: CTA per parent box, thread per (child c, output coefficient k).  The
@@ -1565,7 +1567,8 @@ int fmm_plan_create(mms_ctx *ctx)
         MMS_TRY(far_prepare(ctx, pl));
     {
         // P2M with W staged and the fused parent M2M: at most 160 KB
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     }
     {
         const size_t tsz = 4 * cstride;
@@ -1714,14 +1717,19 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         const long long leaf_off = pl->lev_off[f.L];
         const int up = p2m_up(pl);
         const int rows = up ? 2 : 1;
-        const size_t extra = up ? tsz + (BB / 2) * (4 * (size_t)f.NR + 4 * (size_t)KT) : 0;
+        const int PB = (up && f.s >= 8) ? 4 : BB;
+        const size_t extra = up ? tsz + (PB / 2) * (4 * (size_t)f.NR + 4 * (size_t)KT) : 0;
         const int wsm =
-            (f.C * f.NR) % 4 == 0 && ((size_t)f.C * (rows * BB + f.NR) + extra) * sizeof(float) <= 160 * 1024;
-        const size_t smem = ((size_t)f.C * (rows * BB + (wsm ? f.NR : 0)) + extra) * sizeof(float);
-        MMS_CUDA_TRY(launch_k(k_p2m_row, dim3(div_up(nbx, BB), up ? div_up(nby, 2) : nby),
-                              dim3(up ? (BB / 2) * 4 * KT : 128), smem, ctx->stream, rho, (const float *)pl->Wt,
-                              pl->Mall, leaf_off, f, wsm, up, (const float *)pl->Tm2m,
-                              up ? pl->lev_off[f.L - 1] : 0LL));
+            (f.C * f.NR) % 4 == 0 && ((size_t)f.C * (rows * PB + f.NR) + extra) * sizeof(float) <= 160 * 1024;
+        const size_t smem = ((size_t)f.C * (rows * PB + (wsm ? f.NR : 0)) + extra) * sizeof(float);
+        const dim3 grid(div_up(nbx, PB), up ? div_up(nby, 2) : nby), block(up ? (PB / 2) * 4 * KT : 128);
+        if (PB == 4)
+            MMS_CUDA_TRY(launch_k(k_p2m_row<4>, grid, block, smem, ctx->stream, rho, (const float *)pl->Wt, pl->Mall,
+                                  leaf_off, f, wsm, up, (const float *)pl->Tm2m, up ? pl->lev_off[f.L - 1] : 0LL));
+        else
+            MMS_CUDA_TRY(launch_k(k_p2m_row<BB>, grid, block, smem, ctx->stream, rho, (const float *)pl->Wt,
+                                  pl->Mall, leaf_off, f, wsm, up, (const float *)pl->Tm2m,
+                                  up ? pl->lev_off[f.L - 1] : 0LL));
         MMS_LAUNCH_CHECK(ctx);
         break;
     }
