@@ -1022,38 +1022,61 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
 // BF16 alone, below the FMM truncation error for P <= 6).
 __global__ void k_m2l_gather(const float *__restrict__ Mall, __nv_bfloat16 *__restrict__ A0,
                              __nv_bfloat16 *__restrict__ A1, const int4 *__restrict__ rowinfo,
-                             const long long *__restrict__ lev_off, FmmDev f, int K0, int K1, int NBp0, int NBp1)
+                             const long long *__restrict__ lev_off, FmmDev f, int rows, int K0, int K1, int NBp0,
+                             int NBp1)
 {
-    const int r = blockIdx.x, blk = blockIdx.y;
-    const int4 ri = rowinfo[r];
-    const int lev = ri.x, px = ri.y & 1, py = ri.y >> 1, t = ri.z;
-    const int n = 1 << lev, nh = n >> 1;
-    const int tx = 2 * (t % nh) + px, ty = 2 * (t / nh) + py;
-    const int NB = blk ? f.NR - f.NE : f.NE, NBp = blk ? NBp1 : NBp0, K = blk ? K1 : K0;
-    const int boff = blk ? f.NE : 0;
-    __nv_bfloat16 *row = (blk ? A1 : A0) + (long long)r * 3 * K;
-    const long long off = lev_off[lev];
-    for (int e = threadIdx.x; e < 27 * NBp; e += blockDim.x) {
-        const int q = e / NBp, j = e % NBp;
-        // offset q of the class, in the order the operators were packed
-        const int oyi = q / 6, oxi = q % 6;  // 6 x 6 minus the 3 x 3 near block, skipping it
-        int cnt = 0, ox = 0, oy = 0;
+    // the 27 offsets of each parity class in the order the operators were
+    // packed (6 x 6 around the parity position minus the 3 x 3 near block)
+    __shared__ int sox[4][27], soy[4][27];
+    if (threadIdx.x < 4) {
+        const int px = threadIdx.x & 1, py = threadIdx.x >> 1;
+        int cnt = 0;
         for (int yy = 0; yy < 6; yy++)
             for (int xx = 0; xx < 6; xx++) {
                 const int dx = px - 3 + xx, dy = py - 3 + yy;
                 if (max(abs(dx), abs(dy)) < 2) continue;
-                if (cnt == q) { ox = dx; oy = dy; }
+                sox[threadIdx.x][cnt] = dx;
+                soy[threadIdx.x][cnt] = dy;
                 cnt++;
             }
-        (void)oyi; (void)oxi;
-        float v = 0.f;
-        const int sx = tx - ox, sy = ty - oy;
-        if (j < NB && sx >= 0 && sy >= 0 && sx < n && sy < n) v = Mall[(off + (long long)sy * n + sx) * f.NR + boff + j];
-        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-        row[q * NBp + j] = hi;
-        row[K + q * NBp + j] = hi;
-        row[2 * K + q * NBp + j] = lo;
+    }
+    __syncthreads();
+    const int blk = blockIdx.y;
+    const int NB = blk ? f.NR - f.NE : f.NE, NBp = blk ? NBp1 : NBp0, K = blk ? K1 : K0;
+    const int boff = blk ? f.NE : 0;
+    __nv_bfloat16 *A = blk ? A1 : A0;
+    // one thread per run of 8 coefficients of one offset: 16-byte stores of
+    // hi, hi and lo (NBp and K are multiples of 8, rows start 16-B aligned)
+    const int cpq = NBp >> 3, per_row = 27 * cpq;
+    const long long total = (long long)rows * per_row;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / per_row), c = (int)(e % per_row);
+        const int q = c / cpq, j0 = (c % cpq) * 8;
+        const int4 ri = rowinfo[r];
+        const int lev = ri.x, par = ri.y & 3, t = ri.z;
+        const int n = 1 << lev, nh = n >> 1;
+        const int tx = 2 * (t % nh) + (par & 1), ty = 2 * (t / nh) + (par >> 1);
+        const int sx = tx - sox[par][q], sy = ty - soy[par][q];
+        float v[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v[i] = 0.f;
+        if (sx >= 0 && sy >= 0 && sx < n && sy < n) {
+            const float *src = Mall + (lev_off[lev] + (long long)sy * n + sx) * f.NR + boff + j0;
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+                if (j0 + i < NB) v[i] = __ldg(src + i);
+        }
+        __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            hi[i] = __float2bfloat16_rn(v[i]);
+            lo[i] = __float2bfloat16_rn(v[i] - __bfloat162float(hi[i]));
+        }
+        __nv_bfloat16 *row = A + (long long)r * 3 * K + q * NBp + j0;
+        *reinterpret_cast<uint4 *>(row) = *reinterpret_cast<const uint4 *>(hi);
+        *reinterpret_cast<uint4 *>(row + K) = *reinterpret_cast<const uint4 *>(hi);
+        *reinterpret_cast<uint4 *>(row + 2 * K) = *reinterpret_cast<const uint4 *>(lo);
     }
 }
 
@@ -1373,9 +1396,12 @@ int fmm_plan_create(mms_ctx *ctx)
                 for (int k = 0; k < NB; k++) dst[(size_t)j * NB + k] = src[(size_t)j * KP + k];
         }
     const int m2l_mode = ctx->s.m2l_mode;
-    // auto: the FP32 SIMT kernels; at 256x256x3 the tensor-core path measured
-    // slower (materialised gather + a latency-bound 2-stage K loop over few CTAs)
-    pl->m2l_tc = (m2l_mode == 2);
+    // auto: the tensor-core path from P = 6 at leaf <= 4 and from P = 8 at any
+    // leaf, where it measured faster than the FP32 kernels on a 256 x 256 x 3
+    // film (M2L 49 vs 64 us at P = 6 leaf 4; 72 vs 110 and 29 vs 37 us at P = 8
+    // leaf 4 and 8) at little cost in accuracy (phi rel-L2 vs exact 3.35e-5 vs
+    // 3.34e-5 at P = 6, 3.9e-6 vs 3.5e-6 at P = 8); below, the FP32 kernels
+    pl->m2l_tc = m2l_mode == 2 || (m2l_mode == 0 && (P >= 8 || (P >= 6 && f.s <= 4)));
     pl->m2l_resident = !pl->m2l_tc && m2l_res_supported(NR, f.NE);
     // tensor-core M2L operands: B'_{p,b} rows k = [T_hi | T_lo | T_hi] over the
     // class's 27 offsets (q-major, NBp-padded), matching k_m2l_gather's order
@@ -1756,9 +1782,10 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     }
     case 2: {
         if (pl->m2l_tc) {
-            k_m2l_gather<<<dim3(pl->tc_rows, 2), 256, 0, ctx->stream>>>(pl->Mall, pl->tcA[0], pl->tcA[1],
-                                                                      pl->tc_rowinfo, pl->lev_dev, f, pl->tcK[0],
-                                                                      pl->tcK[1], pl->tcNBp[0], pl->tcNBp[1]);
+            const long long runs = (long long)pl->tc_rows * 27 * (std::max(pl->tcNBp[0], pl->tcNBp[1]) / 8);
+            k_m2l_gather<<<dim3((unsigned)div_up(runs, 256), 2), 256, 0, ctx->stream>>>(
+                pl->Mall, pl->tcA[0], pl->tcA[1], pl->tc_rowinfo, pl->lev_dev, f, pl->tc_rows, pl->tcK[0], pl->tcK[1],
+                pl->tcNBp[0], pl->tcNBp[1]);
             MMS_LAUNCH_CHECK(ctx);
             k_m2l_gemm<<<dim3(div_up(pl->tc_maxm, umma::BM), pl->tc_ksplit, 8), 128,
                          sizeof(umma::Smem<64, TC_STAGES>) + 1024, ctx->stream>>>(pl->tc_groups, pl->tc_ksplit,
