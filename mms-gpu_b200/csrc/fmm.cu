@@ -178,10 +178,34 @@ __device__ __forceinline__ void stage_async(float *dst, const float *src, int n)
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// One P2M output: sum over the leaf's C cells of W[c][k] q[c], w = &W[0][k]
+// (row pitch NR), qq = &q[0] (pitch QS).  Four interleaved partial sums
+// (cells c = 0, 1, 2, 3 mod 4) joined as (s0 + s1) + (s2 + s3): four
+// independent FMA chains a quarter as long as one running sum.
+template <int QS>
+__device__ __forceinline__ float p2m_dot(const float *w, int NR, const float *qq, int C)
+{
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+    const int C4 = C & ~3;
+#pragma unroll 2
+    for (int c = 0; c < C4; c += 4) {
+        a0 = fmaf(w[0], qq[0], a0);
+        a1 = fmaf(w[NR], qq[QS], a1);
+        a2 = fmaf(w[2 * NR], qq[2 * QS], a2);
+        a3 = fmaf(w[3 * NR], qq[3 * QS], a3);
+        w += 4 * NR;
+        qq += 4 * QS;
+    }
+    if (C4 < C) a0 = fmaf(w[0], qq[0], a0);
+    if (C4 + 1 < C) a1 = fmaf(w[NR], qq[QS], a1);
+    if (C4 + 2 < C) a2 = fmaf(w[2 * NR], qq[2 * QS], a2);
+    return (a0 + a1) + (a2 + a3);
+}
+
 // P2M of one item = BB leaf boxes of one row: the boxes' charges are staged
 // transposed in shared memory ([cell][box]); thread per (box, coefficient),
-// each output summed over the cells in order.  Wt: [C][NR] weights (shared or
-// global memory).  q: C * BB floats of shared memory.
+// each output by p2m_dot.  Wt: [C][NR] weights (shared or global memory).
+// q: C * BB floats of shared memory.
 __device__ __forceinline__ void p2m_item(const float *__restrict__ rho, const float *Wt, float *q,
                                          float *__restrict__ Mleaf, const FmmDev &f, int by, int bx0)
 {
@@ -194,25 +218,25 @@ __device__ __forceinline__ void p2m_item(const float *__restrict__ rho, const fl
     __syncthreads();
     for (int e = threadIdx.x; e < BB * f.NR; e += blockDim.x) {
         const int b = e / f.NR, k = e % f.NR;
-        float acc = 0.f;
-#pragma unroll 4
-        for (int c = 0; c < f.C; c++) acc = fmaf(Wt[(long long)c * f.NR + k], q[c * BB + b], acc);
+        const float acc = p2m_dot<BB>(Wt + k, f.NR, q + b, f.C);
         if (bx0 + b < f.nb) Mleaf[((long long)by * f.nb + bx0 + b) * f.NR + k] = acc;
     }
     __syncthreads();
 }
 
-__device__ __forceinline__ void m2m_item(float *__restrict__ Mall, const float *Ts, float *Mc, float *red,
-                                         long long off_p, long long off_c, int np, int box, const FmmDev &f, int t,
-                                         int KT, bool valid);
+__device__ __forceinline__ void m2m_reduce(float *__restrict__ Mall, const float *Ts, const float *Mc, float *red,
+                                           long long off_p, int box, const FmmDev &f, int t, int KT, bool valid);
 
-// P2M: CTA = one item (BB leaf boxes of one row).  With up != 0 (NR <= 32)
-// the CTA takes PB boxes of two leaf rows (both in parallel, thread per (row,
-// box, coefficient)) and then forms their PB/2 parents (the M2M of level L-1)
-// with one 4 KT-thread group per parent, reading the children it just wrote;
-// PB/2 x 128 threads.  PB = 8, or 4 at leaf side >= 8 (twice the CTAs where
-// the boxes are large and few).  Per output the same summation order as p2m_item / m2m_item.
-// Shared memory: charges [rows][C][BB], W [C][NR] when wsm, then (up) the M2M
+// P2M: CTA = one item, PB leaf boxes of one row (up == 0) or of two rows
+// (up != 0, NR <= 32), thread per (row, box, coefficient).  The charges are
+// read a row of PB boxes at a time (one warp per cell row, consecutive
+// lanes on consecutive cells) into [rows][C][PB] in shared memory while the
+// weights W (when wsm) and, with up, the M2M operators stream in by cp.async.
+// With up the CTA then forms the PB/2 parents (the M2M of level L-1), one
+// 4 KT-thread group per parent, from the children it keeps in shared memory;
+// (PB/2) 4 KT threads.  PB = 8, or 4 at leaf side >= 8 or NR > 32.  Per output
+// the arithmetic of p2m_item / m2m_item.
+// Shared memory: charges [rows][C][PB], W [C][NR] when wsm, then (up) the M2M
 // operators and the per-parent M2M scratch.
 template <int PB>
 __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, const float *__restrict__ Wg,
@@ -222,46 +246,55 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
     pdl_begin();
     extern __shared__ __align__(16) float q[];
     const int rows = up ? 2 : 1;
-    const float *Wt = Wg;
-    float *tail = q + rows * f.C * PB;
-    if (wsm) {
-        float *Ws = tail;
-        const int n = f.C * f.NR;
-        stage_async(Ws, Wg, n);
-        Wt = Ws;
-        tail += n;
-    }
-    float *Mleaf = Mall + off_leaf * f.NR;
-    const int bx0 = blockIdx.x * PB;
-    if (!up) {
-        if constexpr (PB == BB) p2m_item(rho, Wt, q, Mleaf, f, blockIdx.y, bx0);
-        return;
-    }
     const int NE = f.NE, NO = f.NR - f.NE, s = f.s, CB = f.C * PB;
     const int tsz = 4 * (NE * NE + NO * NO);
     const int KT = ((f.NR + 31) / 32) * 32;
+    const float *Wt = Wg;
+    float *tail = q + rows * CB;
+    // weights and operators: every chunk in flight before the charges load
+    if (wsm) {
+        for (int i = threadIdx.x * 4; i < f.C * f.NR; i += blockDim.x * 4)
+            umma::cp_async16(umma::smem_u32(tail + i), Wg + i, true);
+        Wt = tail;
+        tail += f.C * f.NR;
+    }
     float *Ts = tail, *scr = Ts + tsz;
-    stage_async(Ts, Tm2m, tsz);
-    for (int i = threadIdx.x; i < 2 * CB; i += blockDim.x) {
-        const int r = i / CB, j = i % CB, b = j % PB, c = j / PB;
-        const int x = (bx0 + b) * s + c % s, y = (2 * blockIdx.y + r) * s + (c / s) % s, z = c / (s * s);
-        q[i] = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
+    if (up)
+        for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+            umma::cp_async16(umma::smem_u32(Ts + i), Tm2m + i, true);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    const int bx0 = blockIdx.x * PB, by0 = rows * blockIdx.y;
+    {
+        const int RW = PB * s, nrow = rows * f.Z * s;
+        const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        for (int row = threadIdx.x >> 5; row < nrow; row += nw) {
+            const int yy = row % s, z = (row / s) % f.Z, r = row / (s * f.Z);
+            const int y = (by0 + r) * s + yy;
+            const float *src = rho + ((long long)z * f.Y + y) * f.X + (long long)bx0 * s;
+            float *dst = q + r * CB + (z * s + yy) * s * PB;
+            for (int xx = lane; xx < RW; xx += 32) {
+                const int b = xx / s, cx = xx - b * s;
+                dst[cx * PB + b] = (bx0 * s + xx < f.X && y < f.Y) ? src[xx] : 0.f;
+            }
+        }
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    for (int e = threadIdx.x; e < 2 * PB * f.NR; e += blockDim.x) {
-        const int r = e / (PB * f.NR), rem = e % (PB * f.NR), b = rem / f.NR, k = rem % f.NR;
-        const float *qr = q + r * CB;
-        float acc = 0.f;
-#pragma unroll 4
-        for (int c = 0; c < f.C; c++) acc = fmaf(Wt[(long long)c * f.NR + k], qr[c * PB + b], acc);
-        if (bx0 + b < f.nb) Mleaf[((long long)(2 * blockIdx.y + r) * f.nb + bx0 + b) * f.NR + k] = acc;
-    }
-    __syncthreads();
+    float *Mleaf = Mall + off_leaf * f.NR;
+    // with up, the children's expansions also go to the parents' scratch
     const int np = f.nb >> 1;
+    for (int e = threadIdx.x; e < rows * PB * f.NR; e += blockDim.x) {
+        const int r = e / (PB * f.NR), rem = e % (PB * f.NR), b = rem / f.NR, k = rem % f.NR;
+        const float acc = p2m_dot<PB>(Wt + k, f.NR, q + r * CB + b, f.C);
+        if (bx0 + b < f.nb) Mleaf[((long long)(by0 + r) * f.nb + bx0 + b) * f.NR + k] = acc;
+        if (up) scr[(b >> 1) * (4 * f.NR + 4 * KT) + ((b & 1) | (r << 1)) * f.NR + k] = acc;
+    }
+    if (!up) return;
+    __syncthreads();
     const int grp = threadIdx.x / (4 * KT), t = threadIdx.x % (4 * KT);
     const int pc = (bx0 >> 1) + grp;
     float *Mc = scr + grp * (4 * f.NR + 4 * KT), *red = Mc + 4 * f.NR;
-    m2m_item(Mall, Ts, Mc, red, off_par, off_leaf, np, blockIdx.y * np + pc, f, t, KT, grp < PB / 2 && pc < np);
+    m2m_reduce(Mall, Ts, Mc, red, off_par, blockIdx.y * np + pc, f, t, KT, grp < PB / 2 && pc < np);
 }
 
 // M2M: CTA per parent box, thread per (child c, output coefficient k).  The
@@ -275,19 +308,12 @@ __device__ __forceinline__ int blk_base(int c, int NE, int NO, int blk)
 
 // one parent box of M2M with a group of 4 KT threads (t = thread in group):
 // thread (child c, coefficient k); Ts = the 4 child operators in shared
-// memory; Mc (4 NR) and red (4 KT) are the group's shared scratch
-__device__ __forceinline__ void m2m_item(float *__restrict__ Mall, const float *Ts, float *Mc, float *red,
-                                         long long off_p, long long off_c, int np, int box, const FmmDev &f, int t,
-                                         int KT, bool valid = true)
+// memory; Mc (4 NR: the children's expansions, child c = (cy & 1) 2 +
+// (cx & 1)) and red (4 KT) are the group's shared scratch
+__device__ __forceinline__ void m2m_reduce(float *__restrict__ Mall, const float *Ts, const float *Mc, float *red,
+                                           long long off_p, int box, const FmmDev &f, int t, int KT, bool valid)
 {
     const int NE = f.NE, NO = f.NR - f.NE;
-    const int bx = box % np, by = box / np, nc = 2 * np;
-    for (int i = t; valid && i < 4 * f.NR; i += 4 * KT) {
-        const int c = i / f.NR, j = i % f.NR;
-        const int cx = 2 * bx + (c & 1), cy = 2 * by + (c >> 1);
-        Mc[i] = Mall[(off_c + (long long)cy * nc + cx) * f.NR + j];
-    }
-    __syncthreads();
     const int c = t / KT, k = t % KT;
     float acc = 0.f;
     if (k < f.NR) {
@@ -302,6 +328,21 @@ __device__ __forceinline__ void m2m_item(float *__restrict__ Mall, const float *
     if (valid && c == 0 && k < f.NR)
         Mall[(off_p + box) * f.NR + k] = (red[k] + red[KT + k]) + (red[2 * KT + k] + red[3 * KT + k]);
     __syncthreads();
+}
+
+// m2m_reduce with the children's expansions read from Mall first
+__device__ __forceinline__ void m2m_item(float *__restrict__ Mall, const float *Ts, float *Mc, float *red,
+                                         long long off_p, long long off_c, int np, int box, const FmmDev &f, int t,
+                                         int KT, bool valid = true)
+{
+    const int bx = box % np, by = box / np, nc = 2 * np;
+    for (int i = t; valid && i < 4 * f.NR; i += 4 * KT) {
+        const int c = i / f.NR, j = i % f.NR;
+        const int cx = 2 * bx + (c & 1), cy = 2 * by + (c >> 1);
+        Mc[i] = Mall[(off_c + (long long)cy * nc + cx) * f.NR + j];
+    }
+    __syncthreads();
+    m2m_reduce(Mall, Ts, Mc, red, off_p, box, f, t, KT, valid);
 }
 
 __global__ void k_m2m_c(float *__restrict__ Mall, const float *__restrict__ Tb, long long off_p, long long off_c,
@@ -907,62 +948,26 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
     const int by = blockIdx.y, bx0 = blockIdx.x * BB;
     const int haspar = pmode != 0;
     const int np = f.nb >> 1, prow = by >> 1;
+    // every global read that does not depend on another goes out first: the
+    // L2L operators (cp.async), the grandparents' locals, partial 0 of this
+    // thread's first parent and leaf M2L partials and its near-field values
+    // (registers); the sums below keep their order (operator term, then
+    // partial 0, 1, ..)
     if (haspar) {
         const int tsz = 4 * (NE * NE + NO * NO);
-        stage_async(Ts, Tl2l, tsz);
+        for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
+            umma::cp_async16(umma::smem_u32(Ts + i), Tl2l + i, true);
     }
-    if (pmode == 1) {
-        for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
-            const int pb = (bx0 >> 1) + i / f.NR;
-            Lp[i] = (pb < np) ? Lpar[((long long)prow * np + pb) * f.NR + i % f.NR] : 0.f;
-        }
-    } else if (pmode >= 2) {
-        const int ng = np >> 1, g0 = bx0 >> 2;
-        if (pmode == 2)
-            for (int i = threadIdx.x; i < GB * f.NR; i += blockDim.x) {
-                const int gc = g0 + i / f.NR;
-                Lg[i] = (gc < ng) ? Lgp[((long long)(prow >> 1) * ng + gc) * f.NR + i % f.NR] : 0.f;
-            }
-        __syncthreads();
-        for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
-            const int pc = (bx0 >> 1) + i / f.NR, k = i % f.NR;
-            float v = 0.f;
-            if (pc < np) {
-                if (pmode == 2) {
-                    const int c = (pc & 1) | ((prow & 1) << 1);
-                    const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
-                    const float *T = Ts + blk_base(c, NE, NO, blk);
-                    const float *lg = Lg + ((pc >> 1) - g0) * f.NR + boff;
-                    float acc = 0.f;
-#pragma unroll 8
-                    for (int j = 0; j < NB; j++) acc = fmaf(T[j * NB + kk], lg[j], acc);
-                    v = acc;
-                }
-                const long long pbox = (long long)prow * np + pc;
-                for (int q = 0; q < nsplit; q++) v += Lpp[q * part_stride + pbox * f.NR + k];
-            }
-            Lp[i] = v;
-        }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    float ppre, lpre;  // partial 0 of this thread's first parent and leaf item
+    {
+        const int i = threadIdx.x;
+        const int pc = (bx0 >> 1) + i / f.NR, k = i % f.NR;
+        const bool okp = pmode >= 2 && i < (BB / 2) * f.NR && pc < np && nsplit > 0;
+        const bool okl = i < BB * f.NR && bx0 + i / f.NR < f.nb && nsplit > 0;
+        ppre = okp ? Lpp[((long long)prow * np + pc) * f.NR + k] : 0.f;
+        lpre = okl ? Lpart_leaf[((long long)by * f.nb + bx0 + i / f.NR) * f.NR + k] : 0.f;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < BB * f.NR; i += blockDim.x) {
-        const int b = i / f.NR, k = i % f.NR;
-        float v = 0.f;
-        if (bx0 + b < f.nb) {
-            const long long box = (long long)by * f.nb + bx0 + b;
-            if (haspar) {
-                const int c = ((bx0 + b) & 1) | ((by & 1) << 1);
-                const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
-                const float *T = Ts + blk_base(c, NE, NO, blk);
-                const float *lp = Lp + (b >> 1) * f.NR + boff;
-                for (int j = 0; j < NB; j++) v = fmaf(T[j * NB + kk], lp[j], v);
-            }
-            for (int q = 0; q < nsplit; q++) v += Lpart_leaf[q * part_stride + box * f.NR + k];
-        }
-        Lb[i] = v;
-    }
-    __syncthreads();
-    // G thread groups: group g evaluates coefficients [k0, k1) of every target
     const int nt = BB * S * Z;
     const int grp = threadIdx.x / nt, t = threadIdx.x % nt;
     const int b = t / (S * Z), r = t % (S * Z);
@@ -973,6 +978,63 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
     float acc[S];
 #pragma unroll
     for (int i = 0; i < S; i++) acc[i] = (valid && grp == 0 && (bx0 + b) * S + i < f.X) ? near[row + i] : 0.f;
+    if (pmode == 1) {
+        for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
+            const int pb = (bx0 >> 1) + i / f.NR;
+            Lp[i] = (pb < np) ? Lpar[((long long)prow * np + pb) * f.NR + i % f.NR] : 0.f;
+        }
+    } else if (pmode == 2) {
+        const int ng = np >> 1, g0 = bx0 >> 2;
+        for (int i = threadIdx.x; i < GB * f.NR; i += blockDim.x) {
+            const int gc = g0 + i / f.NR;
+            Lg[i] = (gc < ng) ? Lgp[((long long)(prow >> 1) * ng + gc) * f.NR + i % f.NR] : 0.f;
+        }
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    if (pmode >= 2) {
+        const int g0 = bx0 >> 2;
+        for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
+            const int pc = (bx0 >> 1) + i / f.NR, k = i % f.NR;
+            float v = 0.f;
+            if (pc < np) {
+                if (pmode == 2) {
+                    const int c = (pc & 1) | ((prow & 1) << 1);
+                    const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+                    const float *T = Ts + blk_base(c, NE, NO, blk);
+                    const float *lg = Lg + ((pc >> 1) - g0) * f.NR + boff;
+                    float a2 = 0.f;
+#pragma unroll 8
+                    for (int j = 0; j < NB; j++) a2 = fmaf(T[j * NB + kk], lg[j], a2);
+                    v = a2;
+                }
+                const long long pbox = (long long)prow * np + pc;
+                for (int q = 0; q < nsplit; q++)
+                    v += (q == 0 && i == (int)threadIdx.x) ? ppre : Lpp[q * part_stride + pbox * f.NR + k];
+            }
+            Lp[i] = v;
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < BB * f.NR; i += blockDim.x) {
+        const int bb = i / f.NR, k = i % f.NR;
+        float v = 0.f;
+        if (bx0 + bb < f.nb) {
+            const long long box = (long long)by * f.nb + bx0 + bb;
+            if (haspar) {
+                const int c = ((bx0 + bb) & 1) | ((by & 1) << 1);
+                const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+                const float *T = Ts + blk_base(c, NE, NO, blk);
+                const float *lp = Lp + (bb >> 1) * f.NR + boff;
+                for (int j = 0; j < NB; j++) v = fmaf(T[j * NB + kk], lp[j], v);
+            }
+            for (int q = 0; q < nsplit; q++)
+                v += (q == 0 && i == (int)threadIdx.x) ? lpre : Lpart_leaf[q * part_stride + box * f.NR + k];
+        }
+        Lb[i] = v;
+    }
+    __syncthreads();
+    // G thread groups: group g evaluates coefficients [k0, k1) of every target
     const float *Lbb = Lb + b * f.NR;
     const int c0 = lz * S * S + ly * S;
     const int k0 = grp * f.NR / G, k1 = valid ? (grp + 1) * f.NR / G : k0;
@@ -1743,12 +1805,17 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         const long long leaf_off = pl->lev_off[f.L];
         const int up = p2m_up(pl);
         const int rows = up ? 2 : 1;
-        const int PB = (up && f.s >= 8) ? 4 : BB;
+        // item width: 4 boxes where the boxes are large (leaf side >= 8) or
+        // the expansions long (NR > 32), for twice the CTAs; else 8
+        const int PB = (f.s >= 8 || f.NR > 32) ? 4 : BB;
         const size_t extra = up ? tsz + (PB / 2) * (4 * (size_t)f.NR + 4 * (size_t)KT) : 0;
-        const int wsm =
-            (f.C * f.NR) % 4 == 0 && ((size_t)f.C * (rows * PB + f.NR) + extra) * sizeof(float) <= 160 * 1024;
+        // without the parent step, long expansions read W through L1 as they
+        // go instead of staging all of it first
+        const int wsm = (f.C * f.NR) % 4 == 0 &&
+                        ((size_t)f.C * (rows * PB + f.NR) + extra) * sizeof(float) <= 160 * 1024;
         const size_t smem = ((size_t)f.C * (rows * PB + (wsm ? f.NR : 0)) + extra) * sizeof(float);
-        const dim3 grid(div_up(nbx, PB), up ? div_up(nby, 2) : nby), block(up ? (PB / 2) * 4 * KT : 128);
+        const dim3 grid(div_up(nbx, PB), up ? div_up(nby, 2) : nby),
+            block(up ? (PB / 2) * 4 * KT : std::min(512, ((PB * f.NR + 31) / 32) * 32));
         if (PB == 4)
             MMS_CUDA_TRY(launch_k(k_p2m_row<4>, grid, block, smem, ctx->stream, rho, (const float *)pl->Wt, pl->Mall,
                                   leaf_off, f, wsm, up, (const float *)pl->Tm2m, up ? pl->lev_off[f.L - 1] : 0LL));
