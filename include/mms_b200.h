@@ -94,7 +94,11 @@ typedef struct {
                                 level (default, fastest measured), 1 P2M ..
                                 L2L in one cooperative launch with grid
                                 barriers (P <= 4, FP32 M2L); identical bits   */
-    int reserved[3];
+    int near_mode;           /* FMM near field: 0 auto (tensor cores at leaf
+                                side 8 and Z <= 4, else FP32), 1 FP32 SIMT,
+                                2 tensor cores (tcgen05 + TMA, split-BF16
+                                hi/lo products; leaf side 8, Z <= 4 only)     */
+    int reserved[2];
 } mms_solver;
 
 typedef struct mms_ctx mms_ctx;

@@ -26,6 +26,8 @@
 #include <algorithm>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include "fmm_ops.hpp"
@@ -100,6 +102,11 @@ struct FmmPlan {
     int n_res_items = 0;
     long long *lev_dev = nullptr;  // device copy of lev_off
     float *near = nullptr;    // [N] near-field potential (P2P) before L2P adds the far field
+    int p2p_tc = 0;           // 1: near field on the tensor cores (leaf side 8): k_p2p_tc
+    __nv_bfloat16 *ntcT = nullptr;  // [3 dy][C][2 parts (hi, lo)][3 dx][C] near-field operators
+    __nv_bfloat16 *ntcR = nullptr;  // [2][Z][nby][nbx][8][8] BF16 hi, lo of rho, box-major, zero-padded
+    CUtensorMap ntc_map[3];   // TMA maps: rho hi, rho lo (4-D, box-major), operators (2-D)
+    float *near3 = nullptr;   // [3 dy][N] near-field partials of k_p2p_tc, summed by L2P
     cudaStream_t side = nullptr;   // P2P runs here, concurrently with P2M .. L2L
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     size_t bytes = 0;
@@ -166,6 +173,15 @@ __global__ void k_l2p_p2p(const float *__restrict__ rho, const float *__restrict
 
 constexpr int BB = 8;         // leaf boxes per CTA along x in the leaf kernels
 constexpr int NSPLIT = 9;     // M2L offset groups (3 offsets each) -> partial locals
+
+// one float into shared memory by an asynchronous copy; zero when !valid
+// (src must still be a readable address)
+__device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(umma::smem_u32(dst)), "l"(src),
+                 "r"(valid ? 4 : 0)
+                 : "memory");
+}
 
 // Stage n floats (n a multiple of 4, both addresses 16-byte aligned) into
 // shared memory with asynchronous copies, every chunk in flight at once, and
@@ -562,8 +578,12 @@ __device__ __forceinline__ void m2l_res_item(const float *__restrict__ Mall, flo
     __syncthreads();
 }
 
+// Registers: at most 112 for NR <= 30 (P <= 4, no spills), so that one CTA
+// fits beside two k_p2p CTAs of 288 threads x 64 registers; the near field
+// runs concurrently with the M2L and, at 117 registers, the M2L's CTAs waited
+// for the near field's to finish.  256 threads per CTA.
 template <int NR_, int NE_>
-__global__ void __launch_bounds__(32 * RES_WARPS) k_m2l_res(const float *__restrict__ Mall, float *__restrict__ Lout,
+__global__ void __maxnreg__(NR_ <= 30 ? 112 : 255) k_m2l_res(const float *__restrict__ Mall, float *__restrict__ Lout,
                                                             const float *__restrict__ Tc, const int4 *__restrict__ items,
                                                             const long long *__restrict__ lev_off, FmmDev f)
 {
@@ -846,17 +866,31 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
     float *qn = sl;                        // [Z][3S][W]
     float *g = qn + Z * 3 * S * W;         // [Z][2S][2S]
     __shared__ int nzr[384];               // staged source row (z, y) holds charge; Z 3S <= 384 whenever BB S Z <= 512
+    static_assert(W % 4 == 0, "staged rows are scanned as float4");
     const int by = blockIdx.y, bx0 = blockIdx.x * BB;
     const int xs0 = bx0 * S - S, ys0 = by * S - S;
-    for (int i = threadIdx.x; i < Z * 3 * S; i += blockDim.x) nzr[i] = 0;
-    __syncthreads();
+    // charges (zero-filled off the grid) and the near-field table all in
+    // flight at once, then one scan per staged row for charge
     for (int i = threadIdx.x; i < Z * 3 * S * W; i += blockDim.x) {
         const int xx = xs0 + i % W, yy = ys0 + (i / W) % (3 * S), zz = i / (W * 3 * S);
-        const float v = (xx >= 0 && yy >= 0 && xx < f.X && yy < f.Y) ? rho[((long long)zz * f.Y + yy) * f.X + xx] : 0.f;
-        qn[i] = v;
-        if (v != 0.f) nzr[i / W] = 1;  // benign race: every writer stores 1
+        const bool ok = xx >= 0 && yy >= 0 && xx < f.X && yy < f.Y;
+        cp_async4(qn + i, ok ? rho + ((long long)zz * f.Y + yy) * f.X + xx : rho, ok);
     }
-    for (int i = threadIdx.x; i < Z * 4 * S * S; i += blockDim.x) g[i] = Gn[i];
+    for (int i = threadIdx.x * 4; i < Z * 4 * S * S; i += blockDim.x * 4)
+        umma::cp_async16(umma::smem_u32(g + i), Gn + i, true);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    for (int i = threadIdx.x; i < Z * 3 * S; i += blockDim.x) {
+        const float4 *rw = reinterpret_cast<const float4 *>(qn + i * W);
+        bool nz = false;
+#pragma unroll
+        for (int v = 0; v < W / 4; v++) {
+            const float4 u = rw[v];
+            nz |= (u.x != 0.f) | (u.y != 0.f) | (u.z != 0.f) | (u.w != 0.f);
+        }
+        nzr[i] = nz;
+    }
     __syncthreads();
     const int nt = BB * S * Z;
     const int grp = threadIdx.x / nt, t = threadIdx.x % nt;
@@ -913,11 +947,16 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
     }
     const int y = by * S + ly;
     if (bx0 + b >= f.nb || y >= f.Y) return;
+    float *o = out + ((long long)lz * f.Y + y) * f.X + (long long)(bx0 + b) * S;
+    if (S % 4 == 0 && (f.X & 3) == 0 && (bx0 + b) * S + S <= f.X) {  // 16-byte stores
 #pragma unroll
-    for (int i = 0; i < S; i++) {
-        const int x = (bx0 + b) * S + i;
-        if (x < f.X) out[((long long)lz * f.Y + y) * f.X + x] = acc[i];
+        for (int v4 = 0; v4 < S / 4; v4++)
+            reinterpret_cast<float4 *>(o)[v4] = make_float4(acc[4 * v4], acc[4 * v4 + 1], acc[4 * v4 + 2], acc[4 * v4 + 3]);
+        return;
     }
+#pragma unroll
+    for (int i = 0; i < S; i++)
+        if ((bx0 + b) * S + i < f.X) o[i] = acc[i];
 }
 
 // k_l2p: leaf locals (the leaf level's L2L: NSPLIT-summed M2L partials plus
@@ -934,7 +973,8 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
                                               const float *__restrict__ Lpar, const float *__restrict__ Tl2l,
                                               const float *__restrict__ Vt, float *__restrict__ phi, FmmDev f,
                                               long long part_stride, int nsplit, int pmode,
-                                              const float *__restrict__ Lgp, const float *__restrict__ Lpp)
+                                              const float *__restrict__ Lgp, const float *__restrict__ Lpp,
+                                              int nnear, long long near_stride)
 {
     pdl_begin();
     extern __shared__ __align__(16) float sl[];
@@ -976,8 +1016,29 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
     const bool valid = bx0 + b < f.nb && y < f.Y;
     const long long row = ((long long)lz * f.Y + y) * f.X + (long long)(bx0 + b) * S;
     float acc[S];
+    // 16-byte accesses where the row of S cells lies inside the grid on a 16-byte boundary
+    const bool vec = S % 4 == 0 && (f.X & 3) == 0 && (bx0 + b) * S + S <= f.X;
+    // near field, in parts for k_p2p_tc (one per source box row) added in order
+    for (int q = 0; q < nnear; q++) {
+        const float *nq = near + q * near_stride + row;
+        if (vec) {
 #pragma unroll
-    for (int i = 0; i < S; i++) acc[i] = (valid && grp == 0 && (bx0 + b) * S + i < f.X) ? near[row + i] : 0.f;
+            for (int v4 = 0; v4 < S / 4; v4++) {
+                const float4 u = (valid && grp == 0) ? reinterpret_cast<const float4 *>(nq)[v4] : make_float4(0.f, 0.f, 0.f, 0.f);
+                if (q == 0) {
+                    acc[4 * v4] = u.x; acc[4 * v4 + 1] = u.y; acc[4 * v4 + 2] = u.z; acc[4 * v4 + 3] = u.w;
+                } else {
+                    acc[4 * v4] += u.x; acc[4 * v4 + 1] += u.y; acc[4 * v4 + 2] += u.z; acc[4 * v4 + 3] += u.w;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < S; i++) {
+                const float u = (valid && grp == 0 && (bx0 + b) * S + i < f.X) ? nq[i] : 0.f;
+                acc[i] = q == 0 ? u : acc[i] + u;
+            }
+        }
+    }
     if (pmode == 1) {
         for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
             const int pb = (bx0 >> 1) + i / f.NR;
@@ -1069,6 +1130,12 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
             for (int i = 0; i < S; i++) acc[i] += red[((gg - 1) * S + i) * nt + t];
     }
     if (!valid) return;
+    if (vec) {
+#pragma unroll
+        for (int v4 = 0; v4 < S / 4; v4++)
+            reinterpret_cast<float4 *>(phi + row)[v4] = make_float4(acc[4 * v4], acc[4 * v4 + 1], acc[4 * v4 + 2], acc[4 * v4 + 3]);
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < S; i++)
         if ((bx0 + b) * S + i < f.X) phi[row + i] = acc[i];
@@ -1141,6 +1208,262 @@ __global__ void k_m2l_gather(const float *__restrict__ Mall, __nv_bfloat16 *__re
         *reinterpret_cast<uint4 *>(row + 2 * K) = *reinterpret_cast<const uint4 *>(lo);
     }
 }
+
+// ---- tensor-core near field (leaf side 8) ----------------------------------
+// Translation invariance: for a source box offset (dx, dy) in {-1, 0, 1}^2 the
+// near-field coupling of a leaf box's C = 64 Z cells to its neighbour's is one
+// fixed C x C matrix T_(dx,dy), built from the near-field table Gn.  For one
+// offset the near field of every leaf box is a GEMM:
+//   phi_(dx,dy)[box][t] = sum_s R[box + (dx, dy)][s] T_(dx,dy)[t][s].
+// Both operands are split into BF16 hi + lo and the tensor cores add
+// R_hi T_hi + R_lo T_hi + R_hi T_lo in FP32 (relative error ~2^-16 per
+// product).  CTA = 4 x 32 boxes x one source box row dy: M = 128 boxes, N = C
+// target cells (<= 256), K = 3 C in steps of one (dx, source layer); each operand
+// tile is one TMA copy in the 128-byte-swizzled layout the MMA reads: the
+// charges from box-major BF16 hi / lo copies of rho (one leaf box layer = one
+// 128-byte row), the operator rows from T.  The three source box rows'
+// partials go to separate buffers that L2P adds in a fixed order.  Few CTAs
+// (three per 128 boxes), so the far-field chain that runs beside it keeps
+// most SMs.
+constexpr int NTC_STAGES = 2;
+
+template <int BN>
+struct NtcSmem {
+    alignas(1024) uint8_t ahi[NTC_STAGES][umma::BM * 128];
+    alignas(1024) uint8_t alo[NTC_STAGES][umma::BM * 128];
+    alignas(1024) uint8_t bhi[NTC_STAGES][BN * 128];
+    alignas(1024) uint8_t blo[NTC_STAGES][BN * 128];
+    uint64_t full[NTC_STAGES];  // the stage's four TMA copies landed
+    uint64_t done[NTC_STAGES];  // the MMAs reading the stage finished
+    uint32_t tmem;
+    int err;
+    int last;                   // last step whose MMAs were committed (-1: none)
+};
+
+__device__ int g_p2p_tc_err;
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(umma::smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// TMA tile loads into shared memory (no multicast), completing on an mbarrier
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int c0, int c1, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+            umma::smem_u32(dst)),
+        "l"((uint64_t)tm), "r"(c0), "r"(c1), "r"(umma::smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(umma::smem_u32(dst)),
+        "l"((uint64_t)tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(umma::smem_u32(bar))
+        : "memory");
+}
+
+// zero-padded BF16 hi / lo copies of rho, box-major: [Z][nby][nbx][8 y][8 x],
+// so that one layer of one leaf box is one 128-byte row of a TMA tile
+__global__ void k_rho_split(const float *__restrict__ rho, __nv_bfloat16 *__restrict__ hi,
+                            __nv_bfloat16 *__restrict__ lo, FmmDev f, int nbx, int nby)
+{
+    pdl_begin();
+    const int n = f.Z * nby * nbx * 64;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int bz = i >> 6, box = bz % (nbx * nby), z = bz / (nbx * nby);
+        const int x = (box % nbx) * 8 + (i & 7), y = (box / nbx) * 8 + ((i >> 3) & 7);
+        const float v = (x < f.X && y < f.Y) ? rho[((long long)z * f.Y + y) * f.X + x] : 0.f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        hi[i] = h;
+        lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
+
+// T'[dy][t][k'] for t < C, k' = part * 3C + dx * C + cell; part 0 hi, 1 lo
+__global__ void k_build_ntc(const float *__restrict__ Gn, __nv_bfloat16 *__restrict__ T, int Z)
+{
+    const int C = 64 * Z, K3 = 3 * C, Kp = 2 * K3;
+    const long long n = 3LL * C * Kp;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int kp = (int)(i % Kp), t = (int)((i / Kp) % C), dy = (int)(i / ((long long)Kp * C)) - 1;
+        const int rem = kp % K3, dxo = rem / C - 1, sc = rem % C;
+        const int tz = t >> 6, ty = (t >> 3) & 7, tx = t & 7;
+        const int sz = sc >> 6, sy = (sc >> 3) & 7, sx = sc & 7;
+        const int ax = abs(tx - sx - 8 * dxo), ay = abs(ty - sy - 8 * dy), az = abs(tz - sz);
+        const float g = Gn[(az * 16 + ay) * 16 + ax];
+        const __nv_bfloat16 hi = __float2bfloat16_rn(g);
+        T[i] = (kp / K3 == 1) ? __float2bfloat16_rn(g - __bfloat162float(hi)) : hi;
+    }
+}
+
+template <int BN>
+size_t ntc_smem() { return 1024 + sizeof(NtcSmem<BN>); }
+
+constexpr int NTC_TW = 32, NTC_TH = 4;  // CTA tile: 4 box rows x 32 boxes = the MMA's 128 rows
+
+// grid (ceil(nbx / 32) x ceil(nby / 4), 3 dy); 128 threads; BN = C = 64 Z.
+// Each CTA sums, for its 4 x 32 boxes, the source boxes in box row dy: one
+// step per (dx, source layer sz) brings in four TMA tiles (the source boxes'
+// layer-sz charges hi and lo, from the box-major copies, off-grid boxes read
+// as zero; the operator columns hi and lo of (dx, sz)) and issues R_hi T_hi
+// + R_lo T_hi + R_hi T_lo.  Its partial goes to [3 dy][N].  Thread 0 keeps
+// NTC_STAGES steps in flight and issues the MMAs.
+template <int BN>
+__global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensorMap tm_hi,
+                                                const __grid_constant__ CUtensorMap tm_lo,
+                                                const __grid_constant__ CUtensorMap tm_T, float *__restrict__ near3,
+                                                FmmDev f, int nbx, int nby, long long ncell)
+{
+    pdl_begin();
+    extern __shared__ uint8_t raw_ntc[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)raw_ntc + 1023) & ~(uintptr_t)1023);
+    NtcSmem<BN> &s = *reinterpret_cast<NtcSmem<BN> *>(base);
+    constexpr int C = BN, K3 = 3 * C;
+    constexpr int TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;  // allocation: a power of two
+    constexpr uint32_t TX = 2 * (umma::BM + BN) * 128;  // bytes per step
+    const int nk = 3 * f.Z;                             // steps: (dx, source layer)
+    const int colt = (nbx + NTC_TW - 1) / NTC_TW;
+    const int bx0 = (blockIdx.x % colt) * NTC_TW, by0 = (blockIdx.x / colt) * NTC_TH;
+    const int dyi = blockIdx.y;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float *out = near3 + (long long)dyi * ncell;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(umma::smem_u32(&s.tmem)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int i = 0; i < NTC_STAGES; i++) {
+            umma::mbar_init(&s.full[i]);
+            umma::mbar_init(&s.done[i]);
+        }
+        s.err = 0;
+        s.last = -1;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = s.tmem;
+    if (tid == 0) {
+        const uint32_t idesc = umma::idesc_bf16(BN);
+        auto issue = [&](int kt) {
+            const int st = kt % NTC_STAGES, dxi = kt / f.Z, sz = kt % f.Z, kc = dxi * C + sz * 64;
+            mbar_expect_tx(&s.full[st], TX);
+            tma_load_4d(s.ahi[st], &tm_hi, 0, bx0 + dxi - 1, by0 + dyi - 1, sz, &s.full[st]);
+            tma_load_4d(s.alo[st], &tm_lo, 0, bx0 + dxi - 1, by0 + dyi - 1, sz, &s.full[st]);
+            tma_load_2d(s.bhi[st], &tm_T, kc, dyi * C, &s.full[st]);
+            tma_load_2d(s.blo[st], &tm_T, K3 + kc, dyi * C, &s.full[st]);
+        };
+        bool ok = true;
+        int issued = 0, landed = 0;
+        for (; issued < NTC_STAGES && issued < nk; issued++) issue(issued);
+        for (int kt = 0; kt < nk && ok; kt++) {
+            const int st = kt % NTC_STAGES;
+            ok = umma::mbar_wait(&s.full[st], (uint32_t)((kt / NTC_STAGES) & 1));
+            if (!ok) break;
+            landed = kt + 1;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t ah = umma::smem_u32(s.ahi[st]), al = umma::smem_u32(s.alo[st]);
+            const uint32_t bh = umma::smem_u32(s.bhi[st]), bl = umma::smem_u32(s.blo[st]);
+#pragma unroll
+            for (int kk = 0; kk < umma::BK / 16; kk++) {
+                umma::mma_bf16(tmem, umma::desc_sw128(ah + kk * 32), umma::desc_sw128(bh + kk * 32), idesc,
+                               (kt > 0 || kk > 0) ? 1u : 0u);
+                umma::mma_bf16(tmem, umma::desc_sw128(al + kk * 32), umma::desc_sw128(bh + kk * 32), idesc, 1u);
+                umma::mma_bf16(tmem, umma::desc_sw128(ah + kk * 32), umma::desc_sw128(bl + kk * 32), idesc, 1u);
+            }
+            umma::mma_commit(&s.done[st]);
+            s.last = kt;
+            // refill the stage of step kt - 1 once its MMAs are done (step kt's run meanwhile)
+            const int prev = kt - 1, nxt = prev + NTC_STAGES;
+            if (prev >= 0 && nxt < nk) {
+                ok = umma::mbar_wait(&s.done[prev % NTC_STAGES], (uint32_t)((prev / NTC_STAGES) & 1));
+                if (ok) issue(issued++);
+            }
+        }
+        // after a timeout: let every copy still in flight land before the CTA's memory goes away
+        for (int kt = landed; kt < issued; kt++) umma::mbar_wait(&s.full[kt % NTC_STAGES], (uint32_t)((kt / NTC_STAGES) & 1));
+        if (!ok) s.err = 1;
+    }
+    __syncthreads();
+    bool ok = s.err == 0;
+    const int last = s.last;
+    // the last commit covers every earlier MMA
+    if (last >= 0) {
+        const bool fin = umma::mbar_wait(&s.done[last % NTC_STAGES], (uint32_t)((last / NTC_STAGES) & 1));
+        ok = ok && fin;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (!ok || last != nk - 1) {
+        if (lane == 0) atomicExch(&g_p2p_tc_err, 1);
+    } else {
+        // warp w holds accumulator rows 32 w .. 32 w + 31 = boxes (bx0 + lane, by0 + w);
+        // 16 columns = two cell rows of one layer: 16-byte stores where the
+        // box's 8 cells lie inside the grid on a 16-byte boundary
+        const int bx = bx0 + lane, by = by0 + warp;
+        const bool okb = bx < nbx && by < nby;
+        const bool vec = (f.X & 3) == 0 && bx * 8 + 8 <= f.X;
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float v[16];
+            umma::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (!okb) continue;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int t = c0 + 8 * h, tz = t >> 6, y = by * 8 + ((t >> 3) & 7);
+                if (y >= f.Y) continue;
+                float *o = out + ((long long)tz * f.Y + y) * f.X + bx * 8;
+                if (vec) {
+                    reinterpret_cast<float4 *>(o)[0] = make_float4(v[8 * h], v[8 * h + 1], v[8 * h + 2], v[8 * h + 3]);
+                    reinterpret_cast<float4 *>(o)[1] = make_float4(v[8 * h + 4], v[8 * h + 5], v[8 * h + 6], v[8 * h + 7]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; i++)
+                        if (bx * 8 + i < f.X) o[i] = v[8 * h + i];
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS) : "memory");
+}
+
+// TMA descriptor of a BF16 tensor (dims / box innermost first, byte strides of dims 1..)
+int ntc_tensor_map(CUtensorMap *tm, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
+                   const cuuint32_t *box)
+{
+    static PFN_cuTensorMapEncodeTiled encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            mms_set_error("tensor-core near field: cuTensorMapEncodeTiled unavailable");
+            return MMS_ERR_CUDA;
+        }
+        encode = (PFN_cuTensorMapEncodeTiled)fn;
+    }
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank, base, dims, strides, box, es,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        mms_set_error("tensor-core near field: tensor map encoding failed (%d)", (int)r);
+        return MMS_ERR_ARG;
+    }
+    return MMS_OK;
+}
+
+#define MMS_NTC_CASES(X) X(64) X(128) X(192) X(256)
 
 __device__ int g_m2l_tc_err;
 
@@ -1274,17 +1597,19 @@ int p2p_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float 
 
 int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float *Lpart_leaf, const float *Lpar,
                const float *Tl2l, const float *Vt, float *phi, long long part_stride, int nsplit, int pmode,
-               const float *Lgp, const float *Lpp, cudaStream_t st)
+               const float *Lgp, const float *Lpp, int nnear, long long near_stride, cudaStream_t st)
 {
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
 #define X(S_, B_)                                                                                              \
     if (f.s == S_) {                                                                                           \
         if (leaf_groups(f) == 3)                                                                               \
             MMS_CUDA_TRY(launch_k(k_l2p<S_, B_, 3>, grid, dim3(3 * leaf_threads(f)), l2p_smem(f), st, near,      \
-                                  Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp));     \
+                                  Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp, nnear, \
+                                  near_stride));                                                           \
         else                                                                                                   \
             MMS_CUDA_TRY(launch_k(k_l2p<S_, B_, 1>, grid, dim3(leaf_threads(f)), l2p_smem(f), st, near, Lpart_leaf, \
-                                  Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp));                \
+                                  Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp, nnear,        \
+                                  near_stride));                                                           \
         return MMS_OK;                                                                                         \
     }
     MMS_LEAF_CASES(X)
@@ -1333,6 +1658,31 @@ int m2l_res_launch(const FmmDev &f, int nitems, const float *Mall, float *Lout, 
 #undef X
     mms_set_error("no resident M2L kernel for NR=%d", f.NR);
     return MMS_ERR_ARG;
+}
+
+// One shared-memory carveout (the largest) for every kernel of the potential.
+// An SM changes its L1 / shared-memory split only when idle, so kernels with
+// different splits cannot share it: the near field, which runs beside the
+// far-field chain, and the chain's kernels would otherwise take turns on the
+// SMs, and a programmatic early launch could not overlap its predecessor.
+int fmm_set_carveout()
+{
+    const int c = cudaSharedmemCarveoutMaxShared;
+    const void *k[] = {(const void *)k_p2m_row<4>, (const void *)k_p2m_row<BB>, (const void *)k_m2m_c,
+                       (const void *)k_top_m2m,    (const void *)k_top_l2l,     (const void *)k_l2l_c,
+                       (const void *)k_m2l_split,  (const void *)k_m2l_gather,  (const void *)k_m2l_gemm};
+    for (const void *fn : k) MMS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, c));
+#define X(a, b) MMS_CUDA_TRY(cudaFuncSetAttribute(k_m2l_res<a, b>, cudaFuncAttributePreferredSharedMemoryCarveout, c));
+    MMS_M2L_RES_CASES(X)
+#undef X
+#define X(S_, B_)                                                                                            \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2p<S_, B_, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, c)); \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2p<S_, B_, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, c)); \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_l2p<S_, B_, 1>, cudaFuncAttributePreferredSharedMemoryCarveout, c)); \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_l2p<S_, B_, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, c));
+    MMS_LEAF_CASES(X)
+#undef X
+    return MMS_OK;
 }
 }  // namespace
 
@@ -1669,6 +2019,7 @@ int fmm_plan_create(mms_ctx *ctx)
 
     }
     if (leaf_threads(f) > 0) MMS_TRY(leaf_set_smem(f));
+    MMS_TRY(fmm_set_carveout());
 
     // algorithmic work of one evaluation (FMA = 2 flops), per stage
     const long long nleafb = (long long)f.nb * f.nb;
@@ -1731,6 +2082,67 @@ int fmm_plan_create(mms_ctx *ctx)
     pl->flops = fl;
     pl->p2p_pairs = pairs;
     pl->m2l_pairs = m2l_pairs;
+    // near field on the tensor cores (k_p2p_tc) at leaf side 8 with a far field
+    // and Z <= 4, by default (near_mode 0) or on request (2); FP32 k_p2p
+    // otherwise.  At 256 x 256 x 3 (P = 4) it took the RK4 step from 224 to
+    // 191 us: its 24 CTAs leave the SMs' FMA and load pipes to the far-field
+    // chain that runs beside it, where k_p2p's 256 CTAs competed with it.
+    const int nmode = ctx->s.near_mode;
+    const bool ntc_ok = s == 8 && leaf_threads(f) > 0 && f.L >= 2 && Z <= 4;
+    if (nmode < 0 || nmode > 2 || (nmode == 2 && !ntc_ok)) {
+        fmm_plan_destroy(ctx);
+        if (nmode < 0 || nmode > 2)
+            mms_set_error("near_mode must be 0 (auto), 1 (FP32) or 2 (tensor cores), got %d", nmode);
+        else
+            mms_set_error("tensor-core near field needs leaf side 8, at least 2 levels and Z <= 4");
+        return MMS_ERR_ARG;
+    }
+    if (ntc_ok && nmode != 1) {
+        const int C = 64 * Z;
+        const int nbx = std::min(f.nb, (f.X + s - 1) / s), nby = std::min(f.nb, (f.Y + s - 1) / s);
+        const size_t nT = 3 * (size_t)C * 6 * C, nR = 2 * (size_t)Z * 64 * nbx * nby;
+        if (cudaMalloc((void **)&pl->ntcT, nT * sizeof(__nv_bfloat16)) != cudaSuccess ||
+            cudaMalloc((void **)&pl->ntcR, nR * sizeof(__nv_bfloat16)) != cudaSuccess ||
+            cudaMalloc((void **)&pl->near3, 3 * (size_t)ctx->N * sizeof(float)) != cudaSuccess) {
+            fmm_plan_destroy(ctx);
+            mms_set_error("FMM plan: device allocation failed");
+            return MMS_ERR_NOMEM;
+        }
+        pl->bytes += (nT + nR) * sizeof(__nv_bfloat16) + 3 * (size_t)ctx->N * sizeof(float);
+        k_build_ntc<<<296, 256, 0, ctx->stream>>>(pl->Gn, pl->ntcT, Z);
+        MMS_LAUNCH_CHECK(ctx);
+        {
+            // charges: [Z][nby][nbx][64] BF16 (hi, then lo), tiles of 1 x 4 x 32 x 64;
+            // operators: [3 C][9 C] BF16, tiles of C x 64
+            const cuuint64_t dR[4] = {64, (cuuint64_t)nbx, (cuuint64_t)nby, (cuuint64_t)Z};
+            const cuuint64_t sR[3] = {128, (cuuint64_t)nbx * 128, (cuuint64_t)nbx * nby * 128};
+            const cuuint32_t bR[4] = {64, NTC_TW, NTC_TH, 1};
+            const cuuint64_t dT[2] = {(cuuint64_t)6 * C, (cuuint64_t)3 * C};
+            const cuuint64_t sT[1] = {(cuuint64_t)6 * C * 2};
+            const cuuint32_t bT[2] = {64, (cuuint32_t)C};
+            int e = ntc_tensor_map(&pl->ntc_map[0], pl->ntcR, 4, dR, sR, bR);
+            if (e == MMS_OK) e = ntc_tensor_map(&pl->ntc_map[1], pl->ntcR + nR / 2, 4, dR, sR, bR);
+            if (e == MMS_OK) e = ntc_tensor_map(&pl->ntc_map[2], pl->ntcT, 2, dT, sT, bT);
+            if (e != MMS_OK) {
+                char keep[512];
+                strncpy(keep, mms_last_error(), sizeof keep - 1);
+                keep[sizeof keep - 1] = 0;
+                fmm_plan_destroy(ctx);
+                mms_set_error("%s", keep);
+                return e;
+            }
+        }
+#define X(BN_)                                                                                                   \
+    if (C == BN_) {                                                                                              \
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2p_tc<BN_>, cudaFuncAttributeMaxDynamicSharedMemorySize,            \
+                                          (int)ntc_smem<BN_>()));                                                \
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2p_tc<BN_>, cudaFuncAttributePreferredSharedMemoryCarveout,         \
+                                          cudaSharedmemCarveoutMaxShared));                                      \
+    }
+        MMS_NTC_CASES(X)
+#undef X
+        pl->p2p_tc = 1;
+    }
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return MMS_OK;
 }
@@ -1742,7 +2154,7 @@ void fmm_plan_destroy(mms_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Tm2lc, pl->Gn, pl->Mall, pl->Lall, pl->Lpart,
                  pl->m2l_items, pl->res_items, pl->lev_dev, pl->near, pl->tcA[0], pl->tcA[1], pl->tcB, pl->tc_rowmap,
-                 pl->tc_rowinfo, pl->tc_groups, pl->far_sync};
+                 pl->tc_rowinfo, pl->tc_groups, pl->far_sync, pl->ntcT, pl->ntcR, pl->near3};
     for (void *p : b)
         if (p) cudaFree(p);
     if (pl->side) cudaStreamSynchronize(pl->side);
@@ -1777,12 +2189,37 @@ static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
     const int pmode = f.L <= 2 ? 0 : (!l2p_up(pl) ? 1 : (f.L - 1 >= 3 ? 2 : 3));
     const float *Lgp = f.L >= 4 ? pl->Lall + pl->lev_off[f.L - 2] * f.NR : nullptr;
     const float *Lpp = f.L > 2 ? pl->Lpart + pl->lev_off[f.L - 1] * f.NR : nullptr;
-    MMS_TRY(l2p_launch(f, nbx, nby, pl->near, pl->Lpart + pl->lev_off[f.L] * f.NR, Lpar, pl->Tl2l, pl->Vt, phi,
-                       pl->nbox_total * f.NR, nsplit, pmode, Lgp, Lpp, ctx->stream));
+    const float *near = pl->p2p_tc ? pl->near3 : pl->near;
+    MMS_TRY(l2p_launch(f, nbx, nby, near, pl->Lpart + pl->lev_off[f.L] * f.NR, Lpar, pl->Tl2l, pl->Vt, phi,
+                       pl->nbox_total * f.NR, nsplit, pmode, Lgp, Lpp, pl->p2p_tc ? 3 : 1, ctx->N, ctx->stream));
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
 
+
+// near field of the FMM potential into pl->near (k_p2p) or, on the tensor
+// cores, into the three partials pl->near3 (k_p2p_tc)
+static int near_launch(mms_ctx *ctx, const float *rho, cudaStream_t st)
+{
+    FmmPlan *pl = ctx->fmm;
+    const FmmDev &f = pl->d;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    if (!pl->p2p_tc) return p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, st);
+    const long long nR = (long long)f.Z * 64 * nbx * nby;
+    __nv_bfloat16 *rhi = pl->ntcR, *rlo = pl->ntcR + nR;
+    MMS_CUDA_TRY(launch_k(k_rho_split, dim3((unsigned)div_up(nR, 256)), dim3(256), 0, st, rho, rhi, rlo, f, nbx, nby));
+    const dim3 grid((unsigned)(div_up(nbx, NTC_TW) * div_up(nby, NTC_TH)), 3);
+#define X(BN_)                                                                                                  \
+    if (64 * f.Z == BN_) {                                                                                      \
+        MMS_CUDA_TRY(launch_k(k_p2p_tc<BN_>, grid, dim3(128), ntc_smem<BN_>(), st, pl->ntc_map[0], pl->ntc_map[1], \
+                              pl->ntc_map[2], pl->near3, f, nbx, nby, (long long)ctx->N));                     \
+        return MMS_OK;                                                                                          \
+    }
+    MMS_NTC_CASES(X)
+#undef X
+    mms_set_error("tensor-core near field: no kernel for %d layers", f.Z);
+    return MMS_ERR_ARG;
+}
 
 // One stage of the FMM potential: 0 P2M, 1 M2M (all levels), 2 M2L (all
 // levels), 3 L2L (all levels, with the M2L partial sums), 4 L2P + P2P.  Every
@@ -1908,7 +2345,7 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
                 MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, phi, ctx->stream));
                 MMS_LAUNCH_CHECK(ctx);
             } else {
-                MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, ctx->stream));
+                MMS_TRY(near_launch(ctx, rho, ctx->stream));
                 MMS_LAUNCH_CHECK(ctx);
                 MMS_TRY(l2p_launch_far(ctx, rho, phi));
             }
@@ -2018,7 +2455,7 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
     const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
     MMS_CUDA_TRY(cudaEventRecord(pl->ev_fork, ctx->stream));
     MMS_CUDA_TRY(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
-    MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, pl->side));
+    MMS_TRY(near_launch(ctx, rho, pl->side));
     MMS_LAUNCH_CHECK(ctx);
     MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
     if (pl->far_fused)

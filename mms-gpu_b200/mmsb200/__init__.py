@@ -58,7 +58,8 @@ class Params(ctypes.Structure):
 
 class Solver(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("fmm_order", ctypes.c_int), ("fmm_leaf", ctypes.c_int),
-                ("m2l_mode", ctypes.c_int), ("far_mode", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
+                ("m2l_mode", ctypes.c_int), ("far_mode", ctypes.c_int), ("near_mode", ctypes.c_int),
+                ("reserved", ctypes.c_int * 2)]
 
 
 class Controller(ctypes.Structure):
@@ -245,12 +246,14 @@ def make_params(Ms=8.6e5, Aexch=1.3e-11, alpha=0.5, gamma=2.21e5, mu0=4e-7 * np.
 
 
 M2L_AUTO, M2L_SIMT, M2L_TENSOR = 0, 1, 2
+NEAR_AUTO, NEAR_SIMT, NEAR_TENSOR = 0, 1, 2
 FAR_STAGES, FAR_FUSED = 0, 1
 
 
-def make_solver(kind=SOLVER_DIRECT, order=4, leaf=0, m2l_mode=M2L_AUTO, far_mode=FAR_STAGES):
+def make_solver(kind=SOLVER_DIRECT, order=4, leaf=0, m2l_mode=M2L_AUTO, far_mode=FAR_STAGES, near_mode=NEAR_AUTO):
     s = Solver()
     s.kind, s.fmm_order, s.fmm_leaf, s.m2l_mode, s.far_mode = kind, order, leaf, m2l_mode, far_mode
+    s.near_mode = near_mode
     return s
 
 

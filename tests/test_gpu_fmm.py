@@ -136,6 +136,41 @@ def test_tensor_core_m2l(cuda, lib, oracle_mod, P, s):
     assert rel_l2(out[mmsb200.M2L_TENSOR], exact) < rel_l2(out[mmsb200.M2L_SIMT], exact) + 3e-5
 
 
+@pytest.mark.parametrize("X,Y,Z", [(64, 64, 3), (70, 45, 3), (320, 40, 3), (48, 48, 4), (40, 40, 2), (24, 24, 1)])
+def test_tensor_core_near_field(cuda, lib, oracle_mod, X, Y, Z):
+    """the tcgen05 split-BF16 near field (leaf side 8: one GEMM per source box
+    row offset, three partials added by L2P) agrees with the FP32 k_p2p to
+    2e-5 relative, on ragged grids, box rows longer than one 32-box CTA and
+    1 to 4 layers, and keeps the FMM within its bound of the exact sum"""
+    import mmsb200
+    d = (5e-9, 5e-9, 5e-9)
+    if Z >= 3:
+        g, rho = film_rho(oracle_mod, X, Y, Z, d, X + 7 * Y + Z, masked=0.3)
+    else:  # too thin for a film with empty caps: random charges
+        rng = np.random.default_rng(X + Y)
+        g = oracle_mod.Grid(X, Y, Z, *d)
+        rho = (rng.standard_normal((Z, Y, X)) * (rng.random((Z, Y, X)) < 0.5) * 1e6).astype(np.float32)
+    out = {}
+    for mode in (mmsb200.NEAR_SIMT, mmsb200.NEAR_TENSOR):
+        with mmsb200.Context(mmsb200.Grid(X, Y, Z, *d), mmsb200.make_params(),
+                             mmsb200.make_solver(mmsb200.SOLVER_FMM, 4, 8, mmsb200.M2L_SIMT,
+                                                 mmsb200.FAR_STAGES, mode)) as ctx:
+            out[mode] = ctx.potential_host(rho)
+            out[mode] = ctx.potential_host(rho)  # a second call reuses the partial buffers
+    assert rel_l2(out[mmsb200.NEAR_TENSOR], out[mmsb200.NEAR_SIMT]) < 2e-5
+    if X * Y * Z <= 64 * 64 * 3:
+        exact = oracle_mod.potential_direct(g, rho)
+        assert rel_l2(out[mmsb200.NEAR_TENSOR], exact) < rel_l2(out[mmsb200.NEAR_SIMT], exact) + 2e-5
+
+
+def test_tensor_core_near_field_needs_leaf_8(cuda, lib):
+    import mmsb200
+    with pytest.raises(Exception, match="leaf side 8"):
+        mmsb200.Context(mmsb200.Grid(64, 64, 3, 5e-9, 5e-9, 5e-9), mmsb200.make_params(),
+                        mmsb200.make_solver(mmsb200.SOLVER_FMM, 4, 4, mmsb200.M2L_SIMT, mmsb200.FAR_STAGES,
+                                            mmsb200.NEAR_TENSOR))
+
+
 def test_autotune_meets_target(cuda, lib, oracle_mod):
     """the autotuner's pick reaches its error target against the FP64 sum, and
     a second call is answered from the cache with the same solver"""
