@@ -463,6 +463,16 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
     return out
 
 
+def bf16_peak():
+    """dense BF16 tensor peak (TFLOP/s): the measured burst figure of this
+    pool's B200s, else the earlier pool measurement"""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["bf16_tflops"]), "measured cuBLAS BF16 GEMM burst (MEASURED_PEAKS.json), of measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "earlier cuBLAS BF16 measurement on this pool, of fallback"
+
+
 def near_pairs_occupied(rho, X, Y, Z, s):
     """near-field (target, source) pairs of the FMM with leaf side s, counting
     only sources with non-zero charge: per leaf box, its cells times the
@@ -503,7 +513,19 @@ def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):
             "unit": "TFLOP/s",
             "peak_source": "measured FP32 FMA microbenchmark (mms_diag_fma_tflops), of measured"}
     roof["achieved"] = st["stage_flops"][dom] / (times[dom] * 1e-3) / 1e12 if times[dom] > 0 else 0.0
-    roof["frac"] = roof["achieved"] / fma_peak
+    if dom == "l2p_p2p" and st["near_tc"]:
+        # near field on the tensor cores: its algorithmic flops (2 per charged
+        # pair) over the stage time, which also holds the FP32 L2P
+        peak, src = bf16_peak()
+        roof.update({"kernel": "k_rho_split + k_p2p_tc + k_l2p (FMM stage l2p_p2p: tcgen05 near field, then L2P)",
+                     "bound": "tensor", "peak": peak, "peak_source": src,
+                     "achieved": 2.0 * occ_pairs / (times[dom] * 1e-3) / 1e12,
+                     "issued_tensor_tflops": 3 * 2.0 * st["p2p_pairs"] / (times[dom] * 1e-3) / 1e12,
+                     "issued_note": "split-BF16: 3 products per pair, every pair of the 3x3 box neighbourhood "
+                                    "(charged or not), over the same stage time"})
+        roof["frac"] = roof["achieved"] / peak
+    else:
+        roof["frac"] = roof["achieved"] / fma_peak
     roof["stage_ms"] = times
     roof["stage_flops"] = st["stage_flops"]
     roof["whole_potential_tflops"] = st["flops"] / (sum(times.values()) * 1e-3) / 1e12
@@ -513,7 +535,8 @@ def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):
     roof["algorithmic"] = ("near field: 2 flops per (target, source) pair over each leaf box's 3x3 neighbourhood, "
                            "sources = cells with non-zero charge in the timed state, targets = all cells; "
                            "plus 2 NR per cell (L2P) and the leaf kernels' L2L")
-    roof["traffic"] = profile_traffic(f"fmm_{dom}_256x256x3_P{st['order']}_leaf{st['leaf']}")
+    key = f"fmm_{dom}_256x256x3_P{st['order']}_leaf{st['leaf']}" + ("_tc" if dom == "l2p_p2p" and st["near_tc"] else "")
+    roof["traffic"] = profile_traffic(key)
     return roof
 
 

@@ -190,6 +190,12 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
 int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *order, double stage_flops[5],
                  long long *p2p_pairs, long long *m2l_pairs);
 
+/* Which kernels the FMM plan runs: near_tc 1 when the near field is the
+ * tensor-core GEMM (k_p2p_tc), m2l_tc 1 when the M2L is (k_m2l_gemm); 0 for
+ * the FP32 kernels.  Either pointer may be NULL.  No counterpart in the
+ * reference (its FMM has one kernel per stage). */
+int mms_fmm_kernels(const mms_ctx *ctx, int *near_tc, int *m2l_tc);
+
 /* Per-stage device time of the FMM potential (ms per stage, all its levels):
  * [0] P2M, [1] M2M, [2] M2L, [3] L2L, [4] L2P + P2P.  After one full
  * evaluation each stage is re-launched `reps` times back to back between two

@@ -2530,6 +2530,17 @@ extern "C" int mms_fmm_info(const mms_ctx *ctx, int *levels, int *leaf, int *ord
     return MMS_OK;
 }
 
+extern "C" int mms_fmm_kernels(const mms_ctx *ctx, int *near_tc, int *m2l_tc)
+{
+    if (!ctx || !ctx->fmm) {
+        mms_set_error("context has no FMM plan");
+        return MMS_ERR_ARG;
+    }
+    if (near_tc) *near_tc = ctx->fmm->p2p_tc;
+    if (m2l_tc) *m2l_tc = ctx->fmm->m2l_tc;
+    return MMS_OK;
+}
+
 extern "C" int mms_fmm_stage_times(mms_ctx *ctx, const float *rho, float *phi, int reps, double ms[5])
 {
     if (!ctx || !ctx->fmm || !rho || !phi || reps < 1 || !ms) {

@@ -136,6 +136,7 @@ SIGNATURES = {
     "mms_surrogate_stats": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "mms_potential_split_dev": (_I, [_VP, _VP, _VP, _VP]),
+    "mms_fmm_kernels": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "mms_fmm_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D),
                           ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
 }
@@ -188,8 +189,10 @@ def fmm_stats(ctx):
     _check(load().mms_fmm_info(ctx.h, ctypes.byref(L), ctypes.byref(s), ctypes.byref(P), fl,
                                ctypes.byref(pp), ctypes.byref(mp)))
     stages = dict(zip(("p2m", "m2m", "m2l", "l2l", "l2p_p2p"), list(fl)))
+    ntc, mtc = ctypes.c_int(), ctypes.c_int()
+    _check(load().mms_fmm_kernels(ctx.h, ctypes.byref(ntc), ctypes.byref(mtc)))
     return dict(levels=L.value, leaf=s.value, order=P.value, flops=float(sum(fl)), stage_flops=stages,
-                p2p_pairs=pp.value, m2l_pairs=mp.value)
+                p2p_pairs=pp.value, m2l_pairs=mp.value, near_tc=bool(ntc.value), m2l_tc=bool(mtc.value))
 
 
 def fmm_stage_times(ctx, rho, phi, reps=10):
