@@ -106,6 +106,7 @@ struct FmmPlan {
     __nv_bfloat16 *ntcT = nullptr;  // [3 dy][C][2 parts (hi, lo)][3 dx][C] near-field operators
     __nv_bfloat16 *ntcR = nullptr;  // [2][Z][nby][nbx][8][8] BF16 hi, lo of rho, box-major, zero-padded
     CUtensorMap ntc_map[3];   // TMA maps: rho hi, rho lo (4-D, box-major), operators (2-D)
+    const float *split_of = nullptr;  // rho whose BF16 split ntcR holds (written by the divergence)
     float *near3 = nullptr;   // [3 dy][N] near-field partials of k_p2p_tc, summed by L2P
     cudaStream_t side = nullptr;   // P2P runs here, concurrently with P2M .. L2L
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1437,6 +1438,16 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS) : "memory");
 }
 
+// out[i] = sum of n parts of stride ns, in order
+__global__ void k_sum_parts(const float *__restrict__ parts, int n, long long ns, float *__restrict__ out)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    float v = parts[i];
+    for (int q = 1; q < n; q++) v += parts[q * ns + i];
+    out[i] = v;
+}
+
 // TMA descriptor of a BF16 tensor (dims / box innermost first, byte strides of dims 1..)
 int ntc_tensor_map(CUtensorMap *tm, void *base, int rank, const cuuint64_t *dims, const cuuint64_t *strides,
                    const cuuint32_t *box)
@@ -2109,6 +2120,7 @@ int fmm_plan_create(mms_ctx *ctx)
             return MMS_ERR_NOMEM;
         }
         pl->bytes += (nT + nR) * sizeof(__nv_bfloat16) + 3 * (size_t)ctx->N * sizeof(float);
+        MMS_CUDA_TRY(cudaMemsetAsync(pl->ntcR, 0, nR * sizeof(__nv_bfloat16), ctx->stream));
         k_build_ntc<<<296, 256, 0, ctx->stream>>>(pl->Gn, pl->ntcT, Z);
         MMS_LAUNCH_CHECK(ctx);
         {
@@ -2207,7 +2219,11 @@ static int near_launch(mms_ctx *ctx, const float *rho, cudaStream_t st)
     if (!pl->p2p_tc) return p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, st);
     const long long nR = (long long)f.Z * 64 * nbx * nby;
     __nv_bfloat16 *rhi = pl->ntcR, *rlo = pl->ntcR + nR;
-    MMS_CUDA_TRY(launch_k(k_rho_split, dim3((unsigned)div_up(nR, 256)), dim3(256), 0, st, rho, rhi, rlo, f, nbx, nby));
+    // the divergence that produced rho wrote its split already, or k_rho_split does it here
+    if (pl->split_of != rho)
+        MMS_CUDA_TRY(launch_k(k_rho_split, dim3((unsigned)div_up(nR, 256)), dim3(256), 0, st, rho, rhi, rlo, f, nbx,
+                              nby));
+    pl->split_of = nullptr;
     const dim3 grid((unsigned)(div_up(nbx, NTC_TW) * div_up(nby, NTC_TH)), 3);
 #define X(BN_)                                                                                                  \
     if (64 * f.Z == BN_) {                                                                                      \
@@ -2488,6 +2504,23 @@ int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
                           (float)(Ms * ctx->g.dx), pl->ev_join, &ctx->launches);
 }
 
+int fmm_split_target(const mms_ctx *ctx, void **hi, void **lo, int *nbx, int *nby)
+{
+    const FmmPlan *pl = ctx->fmm;
+    if (!pl || !pl->p2p_tc) return 0;
+    const FmmDev &f = pl->d;
+    *nbx = std::min(f.nb, (f.X + f.s - 1) / f.s);
+    *nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    *hi = pl->ntcR;
+    *lo = pl->ntcR + (size_t)f.Z * 64 * *nbx * *nby;
+    return 1;
+}
+
+void fmm_split_written(mms_ctx *ctx, const float *rho)
+{
+    if (ctx->fmm) ctx->fmm->split_of = rho;
+}
+
 // FMM potential and its exact near-field part (for the surrogate's targets)
 int launch_potential_split(mms_ctx *ctx, const float *rho, float *phi, float *near)
 {
@@ -2498,8 +2531,13 @@ int launch_potential_split(mms_ctx *ctx, const float *rho, float *phi, float *ne
     }
     MMS_TRY(launch_potential_fmm(ctx, rho, phi));
     const FmmDev &f = pl->d;
-    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
-    MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, near, ctx->stream));
+    if (pl->p2p_tc) {
+        // the near field the potential used: its three partials, added in L2P's order
+        k_sum_parts<<<(unsigned)div_up((long long)ctx->N, 256), 256, 0, ctx->stream>>>(pl->near3, 3, ctx->N, near);
+    } else {
+        const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+        MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, near, ctx->stream));
+    }
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }

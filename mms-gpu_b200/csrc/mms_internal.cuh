@@ -153,6 +153,13 @@ void sno_set_fast(mms_sno *n, bool fast);
 int rel_l2_dev(mms_ctx *ctx, const float *a, const float *b, long long n, double *out);
 void fmm_plan_destroy(mms_ctx *ctx);
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi);
+// the tensor-core near field's box-major BF16 hi / lo charges, for a
+// divergence kernel to write beside rho: returns 0 when the plan has no
+// tensor-core near field; fmm_split_written(ctx, rho) records that they hold
+// rho's split (a potential of that rho then skips k_rho_split), and
+// fmm_split_written(ctx, nullptr) forgets it
+int fmm_split_target(const mms_ctx *ctx, void **hi, void **lo, int *nbx, int *nby);
+void fmm_split_written(mms_ctx *ctx, const float *rho);
 int fmm_far_error(mms_ctx *ctx);  // 1: a fused far-field barrier timed out
 size_t fmm_plan_bytes(const mms_ctx *ctx);
 

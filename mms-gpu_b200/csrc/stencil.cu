@@ -12,6 +12,8 @@
 //    right-hand side (ode_functions.cpp:11-18) and the RK4 stage combination
 //    (ode_functions.cpp:96-145), so every state array is read once and written
 //    once per stage.
+#include <cuda_bf16.h>
+
 #include "mms_internal.cuh"
 
 #include <math.h>
@@ -142,7 +144,11 @@ __global__ void k_hfield_aos(const float *__restrict__ M, const float *__restric
 
 // ---- FP64 SoA resident state ----------------------------------------------
 
-__global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho, GridK g)
+// rho = div M; with rhi != NULL also the BF16 hi / lo split of rho in the
+// box-major layout of the tensor-core near field ([Z][nby][nbx][8][8], leaf
+// side 8; the padding cells beyond the grid stay zero from the plan)
+__global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho, GridK g,
+                          __nv_bfloat16 *__restrict__ rhi, __nv_bfloat16 *__restrict__ rlo, int nbx, int nby)
 {
     pdl_begin();
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -157,7 +163,14 @@ __global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho,
     double y0 = (y != 0) ? My[i - sy] : 0.0;
     double z2 = (z != g.Z - 1) ? Mz[i + sz] : 0.0;
     double z0 = (z != 0) ? Mz[i - sz] : 0.0;
-    rho[i] = (float)(0.5 * ((x2 - x0) / g.dx + (y2 - y0) / g.dy + (z2 - z0) / g.dz));
+    const float v = (float)(0.5 * ((x2 - x0) / g.dx + (y2 - y0) / g.dy + (z2 - z0) / g.dz));
+    rho[i] = v;
+    if (rhi) {
+        const long long j = (((long long)z * nby + (y >> 3)) * nbx + (x >> 3)) * 64 + (y & 7) * 8 + (x & 7);
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        rhi[j] = h;
+        rlo[j] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
 }
 
 // One RK4 stage (ode_functions.cpp:96-145):
@@ -379,6 +392,7 @@ PhysK mms_ctx::pk() const
 
 int launch_divergence_aos(mms_ctx *ctx, const float *M, float *rho)
 {
+    fmm_split_written(ctx, nullptr);  // rho changes without its BF16 split
     k_div_aos<<<div_up(ctx->N, TPB), TPB, 0, ctx->stream>>>(M, rho, ctx->gk(), (float)ctx->g.dx, (float)ctx->g.dy,
                                                            (float)ctx->g.dz);
     MMS_LAUNCH_CHECK(ctx);
@@ -387,8 +401,13 @@ int launch_divergence_aos(mms_ctx *ctx, const float *M, float *rho)
 
 int launch_divergence_soa(mms_ctx *ctx, const double *M, float *rho)
 {
-    MMS_CUDA_TRY(launch_k(k_div_soa, dim3(div_up(ctx->N, TPB)), dim3(TPB), 0, ctx->stream, M, rho, ctx->gk()));
+    void *hi = nullptr, *lo = nullptr;
+    int nbx = 0, nby = 0;
+    const int split = fmm_split_target(ctx, &hi, &lo, &nbx, &nby);
+    MMS_CUDA_TRY(launch_k(k_div_soa, dim3(div_up(ctx->N, TPB)), dim3(TPB), 0, ctx->stream, M, rho, ctx->gk(),
+                          (__nv_bfloat16 *)(split ? hi : nullptr), (__nv_bfloat16 *)(split ? lo : nullptr), nbx, nby));
     MMS_LAUNCH_CHECK(ctx);
+    fmm_split_written(ctx, split ? rho : nullptr);
     return MMS_OK;
 }
 

@@ -163,6 +163,31 @@ def test_tensor_core_near_field(cuda, lib, oracle_mod, X, Y, Z):
         assert rel_l2(out[mmsb200.NEAR_TENSOR], exact) < rel_l2(out[mmsb200.NEAR_SIMT], exact) + 2e-5
 
 
+def test_potential_split_with_tensor_core_near_field(cuda, lib, oracle_mod):
+    """the split entry point returns the near field the potential used (the
+    tensor-core partials, added in L2P's order): it matches the FP32 near
+    field to 2e-5 and its phi is the ordinary potential's, bit for bit"""
+    import torch
+    import mmsb200
+    X, Y, Z = 96, 64, 3
+    d = (5e-9, 5e-9, 5e-9)
+    g, rho_h = film_rho(oracle_mod, X, Y, Z, d, 5, masked=0.3)
+    rho = torch.from_numpy(rho_h.ravel()).cuda()
+    out = {}
+    for mode in (mmsb200.NEAR_SIMT, mmsb200.NEAR_TENSOR):
+        with mmsb200.Context(mmsb200.Grid(X, Y, Z, *d), mmsb200.make_params(),
+                             mmsb200.make_solver(mmsb200.SOLVER_FMM, 4, 8, mmsb200.M2L_SIMT,
+                                                 mmsb200.FAR_STAGES, mode)) as ctx:
+            phi, near, phi1 = torch.zeros_like(rho), torch.zeros_like(rho), torch.zeros_like(rho)
+            ctx.potential_split_dev(rho, phi, near)
+            ctx.potential_dev(rho, phi1)
+            ctx.sync()
+            out[mode] = (phi.cpu().numpy(), near.cpu().numpy(), phi1.cpu().numpy())
+    phi, near, phi1 = out[mmsb200.NEAR_TENSOR]
+    assert np.array_equal(phi, phi1)
+    assert rel_l2(near, out[mmsb200.NEAR_SIMT][1]) < 2e-5
+
+
 def test_tensor_core_near_field_needs_leaf_8(cuda, lib):
     import mmsb200
     with pytest.raises(Exception, match="leaf side 8"):
