@@ -969,13 +969,18 @@ __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, cons
 //   2  formed here: L2L of the grandparents' final locals (Lgp, level L-2)
 //      plus the parents' M2L partials (Lpp), the order of the L2L pass
 //   3  formed here from the parents' partials alone (parent level 2)
+//   4  as 2, with the grandparents' final locals formed here too: levels
+//      2 .. L-2 of the CTA's ancestors from their M2L partials (Lpart_all,
+//      lev_off), in the order of l2l_top_box / l2l_item, so no L2L launch
+//      precedes L2P
 template <int S, int BB, int G>
 __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, const float *__restrict__ Lpart_leaf,
                                               const float *__restrict__ Lpar, const float *__restrict__ Tl2l,
                                               const float *__restrict__ Vt, float *__restrict__ phi, FmmDev f,
                                               long long part_stride, int nsplit, int pmode,
                                               const float *__restrict__ Lgp, const float *__restrict__ Lpp,
-                                              int nnear, long long near_stride)
+                                              int nnear, long long near_stride, const float *__restrict__ Lpart_all,
+                                              const long long *__restrict__ lev_off)
 {
     pdl_begin();
     extern __shared__ __align__(16) float sl[];
@@ -1054,13 +1059,48 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
+    if (pmode == 4) {
+        // ancestors of the CTA's leaves at levels 2 .. L-2 (at most GB per
+        // level), each level from the one above; Lb is free until the leaf
+        // locals and holds the intermediate levels, level L-2 ends in Lg
+        float *cur = Lb, *nxt = Lb + GB * f.NR;
+        int ax0p = 0;
+        for (int l = 2; l <= f.L - 2; l++) {
+            const int sh = f.L - l, n = 1 << l;
+            const int ax0 = bx0 >> sh, ax1 = (min(bx0 + BB, f.nb) - 1) >> sh, ay = by >> sh;
+            float *dst = (l == f.L - 2) ? Lg : nxt;
+            for (int i = threadIdx.x; i < GB * f.NR; i += blockDim.x) {
+                const int ax = ax0 + i / f.NR, k = i % f.NR;
+                float v = 0.f;
+                if (ax <= ax1) {
+                    const long long box = lev_off[l] + (long long)ay * n + ax;
+                    if (l > 2) {
+                        const int c = (ax & 1) | ((ay & 1) << 1);
+                        const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
+                        const float *T = Ts + blk_base(c, NE, NO, blk);
+                        const float *lp = cur + ((ax >> 1) - ax0p) * f.NR + boff;
+                        float a2 = 0.f;
+#pragma unroll 8
+                        for (int j = 0; j < NB; j++) a2 = fmaf(T[j * NB + kk], lp[j], a2);
+                        v = a2;
+                    }
+                    for (int q = 0; q < nsplit; q++) v += Lpart_all[q * part_stride + box * f.NR + k];
+                }
+                dst[i] = v;
+            }
+            __syncthreads();
+            nxt = cur;
+            cur = dst;
+            ax0p = ax0;
+        }
+    }
     if (pmode >= 2) {
         const int g0 = bx0 >> 2;
         for (int i = threadIdx.x; i < (BB / 2) * f.NR; i += blockDim.x) {
             const int pc = (bx0 >> 1) + i / f.NR, k = i % f.NR;
             float v = 0.f;
             if (pc < np) {
-                if (pmode == 2) {
+                if (pmode == 2 || pmode == 4) {
                     const int c = (pc & 1) | ((prow & 1) << 1);
                     const int blk = k >= NE, NB = blk ? NO : NE, kk = blk ? k - NE : k, boff = blk ? NE : 0;
                     const float *T = Ts + blk_base(c, NE, NO, blk);
@@ -1608,7 +1648,8 @@ int p2p_launch(const FmmDev &f, int nbx, int nby, const float *rho, const float 
 
 int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float *Lpart_leaf, const float *Lpar,
                const float *Tl2l, const float *Vt, float *phi, long long part_stride, int nsplit, int pmode,
-               const float *Lgp, const float *Lpp, int nnear, long long near_stride, cudaStream_t st)
+               const float *Lgp, const float *Lpp, int nnear, long long near_stride, const float *Lpart_all,
+               const long long *lev_off, cudaStream_t st)
 {
     const dim3 grid(div_up(nbx, leaf_bb(f.s)), nby);
 #define X(S_, B_)                                                                                              \
@@ -1616,11 +1657,11 @@ int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float
         if (leaf_groups(f) == 3)                                                                               \
             MMS_CUDA_TRY(launch_k(k_l2p<S_, B_, 3>, grid, dim3(3 * leaf_threads(f)), l2p_smem(f), st, near,      \
                                   Lpart_leaf, Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp, nnear, \
-                                  near_stride));                                                           \
+                                  near_stride, Lpart_all, lev_off));                                       \
         else                                                                                                   \
             MMS_CUDA_TRY(launch_k(k_l2p<S_, B_, 1>, grid, dim3(leaf_threads(f)), l2p_smem(f), st, near, Lpart_leaf, \
                                   Lpar, Tl2l, Vt, phi, f, part_stride, nsplit, pmode, Lgp, Lpp, nnear,        \
-                                  near_stride));                                                           \
+                                  near_stride, Lpart_all, lev_off));                                       \
         return MMS_OK;                                                                                         \
     }
     MMS_LEAF_CASES(X)
@@ -1700,6 +1741,7 @@ int fmm_set_carveout()
 int fmm_default_leaf(int P, int X, int Y);
 int far_prepare(mms_ctx *ctx, FmmPlan *pl);
 static int l2p_up(const FmmPlan *pl);
+static int l2p_top(const FmmPlan *pl);
 static int p2m_up(const FmmPlan *pl);
 
 int fmm_plan_create(mms_ctx *ctx)
@@ -2080,6 +2122,10 @@ int fmm_plan_create(mms_ctx *ctx)
             pl->stage_flops[3] -= m;
             pl->stage_flops[4] += m;
         }
+        if (l2p_top(pl)) {  // every remaining level of the downward pass
+            pl->stage_flops[4] += pl->stage_flops[3];
+            pl->stage_flops[3] = 0;
+        }
         if (p2m_up(pl)) {
             const double m = 2.0 * 4.0 * (double)(1 << (f.L - 1)) * (1 << (f.L - 1)) * blk2;
             pl->stage_flops[1] -= m;
@@ -2187,6 +2233,9 @@ static int l2p_up(const FmmPlan *pl) { return pl->d.L >= 3 && leaf_threads(pl->d
 static int p2m_up(const FmmPlan *pl) { return l2p_up(pl) && pl->d.NR <= 32; }
 // levels 2 and 3 share one launch each way (k_top_m2m / k_top_l2l: 16 KT <= 512 threads)
 static int top_two(const FmmPlan *pl) { return pl->d.NR <= 32 && !pl->far_fused; }
+// L2P also forms levels 2 .. L-2 of each CTA's ancestors (pmode 4): no L2L
+// launch at all between the M2L and L2P
+static int l2p_top(const FmmPlan *pl) { return l2p_up(pl) && pl->d.L >= 4; }
 
 // L2P of the far field onto the near field already in pl->near
 static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
@@ -2198,12 +2247,13 @@ static int l2p_launch_far(mms_ctx *ctx, const float *rho, float *phi)
     const int nsplit = pl->m2l_tc ? pl->tc_ksplit : (pl->m2l_resident ? 1 : NSPLIT);
     const float *Lpar = f.L > 2 ? pl->Lall + pl->lev_off[f.L - 1] * f.NR : nullptr;
     // parents' locals: ready (an L2L pass made level L-1) or formed in the leaf kernel
-    const int pmode = f.L <= 2 ? 0 : (!l2p_up(pl) ? 1 : (f.L - 1 >= 3 ? 2 : 3));
+    const int pmode = f.L <= 2 ? 0 : (!l2p_up(pl) ? 1 : (l2p_top(pl) ? 4 : (f.L - 1 >= 3 ? 2 : 3)));
     const float *Lgp = f.L >= 4 ? pl->Lall + pl->lev_off[f.L - 2] * f.NR : nullptr;
     const float *Lpp = f.L > 2 ? pl->Lpart + pl->lev_off[f.L - 1] * f.NR : nullptr;
     const float *near = pl->p2p_tc ? pl->near3 : pl->near;
     MMS_TRY(l2p_launch(f, nbx, nby, near, pl->Lpart + pl->lev_off[f.L] * f.NR, Lpar, pl->Tl2l, pl->Vt, phi,
-                       pl->nbox_total * f.NR, nsplit, pmode, Lgp, Lpp, pl->p2p_tc ? 3 : 1, ctx->N, ctx->stream));
+                       pl->nbox_total * f.NR, nsplit, pmode, Lgp, Lpp, pl->p2p_tc ? 3 : 1, ctx->N, pl->Lpart,
+                       pl->lev_dev, ctx->stream));
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
@@ -2331,7 +2381,8 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     case 3: {
         // level 2 from its M2L partials, levels 3 .. L-1 one launch each; the
         // leaf level is formed inside the leaf kernel (or by k_l2l_c for the
-        // generic leaf kernel)
+        // generic leaf kernel); with l2p_top the leaf kernel forms them all
+        if (l2p_top(pl)) break;
         const int lend = leaf_threads(f) > 0 ? f.L - 1 - l2p_up(pl) : f.L;
         const int top = top_two(pl) && lend >= 3;
         if (top) {
