@@ -1006,6 +1006,20 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     float ppre, lpre;  // partial 0 of this thread's first parent and leaf item
+    // pmode 4: partial 0 of this thread's ancestor item at levels 2 .. 4 (the
+    // item the level loop below gives it when GB NR <= blockDim)
+    constexpr int NPF = 3;
+    float apre[NPF];
+#pragma unroll
+    for (int u = 0; u < NPF; u++) {
+        apre[u] = 0.f;
+        const int l = 2 + u, i = threadIdx.x;
+        if (pmode == 4 && l <= f.L - 2 && i < GB * f.NR && nsplit > 0) {
+            const int sh = f.L - l, ax = (bx0 >> sh) + i / f.NR;
+            if (ax <= (min(bx0 + BB, f.nb) - 1) >> sh)
+                apre[u] = Lpart_all[(lev_off[l] + (long long)(by >> sh) * (1 << l) + ax) * f.NR + i % f.NR];
+        }
+    }
     {
         const int i = threadIdx.x;
         const int pc = (bx0 >> 1) + i / f.NR, k = i % f.NR;
@@ -1084,7 +1098,18 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
                         for (int j = 0; j < NB; j++) a2 = fmaf(T[j * NB + kk], lp[j], a2);
                         v = a2;
                     }
-                    for (int q = 0; q < nsplit; q++) v += Lpart_all[q * part_stride + box * f.NR + k];
+                    for (int q = 0; q < nsplit; q++) {
+                        float pq;
+                        if (q == 0 && i == (int)threadIdx.x && l - 2 < NPF) {
+                            pq = apre[0];
+#pragma unroll
+                            for (int u = 1; u < NPF; u++)
+                                if (l - 2 == u) pq = apre[u];
+                        } else {
+                            pq = Lpart_all[q * part_stride + box * f.NR + k];
+                        }
+                        v += pq;
+                    }
                 }
                 dst[i] = v;
             }
