@@ -115,6 +115,9 @@ int mms_ctx_create(const mms_grid *grid, const mms_params *params, const mms_sol
 int mms_ctx_destroy(mms_ctx *ctx);
 int mms_ctx_set_params(mms_ctx *ctx, const mms_params *params);
 int mms_ctx_set_solver(mms_ctx *ctx, const mms_solver *solver);
+/* Waits for the context's stream; MMS_ERR_CUDA when a kernel's bounded wait
+ * gave up since the solver was set (fused far-field grid barrier, or the
+ * tensor-core near field / M2L pipeline): its results are then not valid. */
 int mms_ctx_sync(mms_ctx *ctx);
 /* number of kernels this library launched through ctx so far */
 int64_t mms_ctx_kernel_launches(const mms_ctx *ctx);

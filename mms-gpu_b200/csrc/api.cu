@@ -469,7 +469,7 @@ int mms_ctx_sync(mms_ctx *ctx)
     }
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (fmm_far_error(ctx)) {
-        mms_set_error("FMM far field: a grid barrier wait timed out");
+        mms_set_error("FMM: a bounded wait timed out (fused far-field barrier or tensor-core pipeline)");
         return MMS_ERR_CUDA;
     }
     return MMS_OK;

@@ -2226,6 +2226,11 @@ int fmm_plan_create(mms_ctx *ctx)
 #undef X
         pl->p2p_tc = 1;
     }
+    if (pl->p2p_tc || pl->m2l_tc) {  // wait-timeout flags of the tensor-core kernels
+        const int zero = 0;
+        MMS_CUDA_TRY(cudaMemcpyToSymbolAsync(g_p2p_tc_err, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, ctx->stream));
+        MMS_CUDA_TRY(cudaMemcpyToSymbolAsync(g_m2l_tc_err, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, ctx->stream));
+    }
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return MMS_OK;
 }
@@ -2522,13 +2527,26 @@ int far_launch(mms_ctx *ctx, const float *rho)
     return MMS_ERR_ARG;
 }
 
-// 1 when a barrier of the fused far-field kernel timed out since the plan was made
+// 1 when a bounded wait gave up since the plan was made: a grid barrier of the
+// fused far-field kernel, or an mbarrier wait of the tensor-core near field or
+// M2L (their flags are per device and cleared when such a plan is made)
 int fmm_far_error(mms_ctx *ctx)
 {
-    if (!ctx->fmm || !ctx->fmm->far_sync) return 0;
-    FarSync h{};
-    if (cudaMemcpy(&h, ctx->fmm->far_sync, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
-    return h.err != 0;
+    if (!ctx->fmm) return 0;
+    int err = 0;
+    if (ctx->fmm->far_sync) {
+        FarSync h{};
+        if (cudaMemcpy(&h, ctx->fmm->far_sync, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+        err |= h.err != 0;
+    }
+    if (ctx->fmm->p2p_tc || ctx->fmm->m2l_tc) {
+        int a = 0, b = 0;
+        if (cudaMemcpyFromSymbol(&a, g_p2p_tc_err, sizeof a) != cudaSuccess ||
+            cudaMemcpyFromSymbol(&b, g_m2l_tc_err, sizeof b) != cudaSuccess)
+            return 1;
+        err |= (ctx->fmm->p2p_tc && a) || (ctx->fmm->m2l_tc && b);
+    }
+    return err;
 }
 
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)

@@ -160,7 +160,7 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi);
 // fmm_split_written(ctx, nullptr) forgets it
 int fmm_split_target(const mms_ctx *ctx, void **hi, void **lo, int *nbx, int *nby);
 void fmm_split_written(mms_ctx *ctx, const float *rho);
-int fmm_far_error(mms_ctx *ctx);  // 1: a fused far-field barrier timed out
+int fmm_far_error(mms_ctx *ctx);  // 1: a bounded wait of an FMM kernel timed out
 size_t fmm_plan_bytes(const mms_ctx *ctx);
 
 // tcgen05 BF16 GEMM (gemm.cu): C (+)= A B^T, A M x K, B N x K, K-major
