@@ -1291,14 +1291,15 @@ __global__ void k_m2l_gather(const float *__restrict__ Mall, __nv_bfloat16 *__re
 // partials go to separate buffers that L2P adds in a fixed order.  Few CTAs
 // (three per 128 boxes), so the far-field chain that runs beside it keeps
 // most SMs.
-constexpr int NTC_STAGES = 2;
+constexpr int NTC_STAGES = 3;
 
+// BN = C target cells of a box; a CTA takes half of them (N = BN / 2)
 template <int BN>
 struct NtcSmem {
     alignas(1024) uint8_t ahi[NTC_STAGES][umma::BM * 128];
     alignas(1024) uint8_t alo[NTC_STAGES][umma::BM * 128];
-    alignas(1024) uint8_t bhi[NTC_STAGES][BN * 128];
-    alignas(1024) uint8_t blo[NTC_STAGES][BN * 128];
+    alignas(1024) uint8_t bhi[NTC_STAGES][(BN / 2) * 128];
+    alignas(1024) uint8_t blo[NTC_STAGES][(BN / 2) * 128];
     uint64_t full[NTC_STAGES];  // the stage's four TMA copies landed
     uint64_t done[NTC_STAGES];  // the MMAs reading the stage finished
     uint32_t tmem;
@@ -1373,7 +1374,7 @@ size_t ntc_smem() { return 1024 + sizeof(NtcSmem<BN>); }
 
 constexpr int NTC_TW = 32, NTC_TH = 4;  // CTA tile: 4 box rows x 32 boxes = the MMA's 128 rows
 
-// grid (ceil(nbx / 32) x ceil(nby / 4), 3 dy); 128 threads; BN = C = 64 Z.
+// grid (ceil(nbx / 32) x ceil(nby / 4), 3 dy, 2 halves of the target cells); 128 threads; BN = C = 64 Z.
 // Each CTA sums, for its 4 x 32 boxes, the source boxes in box row dy: one
 // step per (dx, source layer sz) brings in four TMA tiles (the source boxes'
 // layer-sz charges hi and lo, from the box-major copies, off-grid boxes read
@@ -1390,13 +1391,13 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
     extern __shared__ uint8_t raw_ntc[];
     uint8_t *base = (uint8_t *)(((uintptr_t)raw_ntc + 1023) & ~(uintptr_t)1023);
     NtcSmem<BN> &s = *reinterpret_cast<NtcSmem<BN> *>(base);
-    constexpr int C = BN, K3 = 3 * C;
-    constexpr int TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;  // allocation: a power of two
-    constexpr uint32_t TX = 2 * (umma::BM + BN) * 128;  // bytes per step
+    constexpr int C = BN, K3 = 3 * C, NH = BN / 2;     // NH target cells per CTA
+    constexpr int TCOLS = NH <= 32 ? 32 : NH <= 64 ? 64 : NH <= 128 ? 128 : 256;  // allocation: a power of two
+    constexpr uint32_t TX = 2 * (umma::BM + NH) * 128;  // bytes per step
     const int nk = 3 * f.Z;                             // steps: (dx, source layer)
     const int colt = (nbx + NTC_TW - 1) / NTC_TW;
     const int bx0 = (blockIdx.x % colt) * NTC_TW, by0 = (blockIdx.x / colt) * NTC_TH;
-    const int dyi = blockIdx.y;
+    const int dyi = blockIdx.y, t0 = blockIdx.z * NH;  // target cells t0 .. t0 + NH - 1
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     float *out = near3 + (long long)dyi * ncell;
     if (warp == 0) {
@@ -1419,14 +1420,14 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = s.tmem;
     if (tid == 0) {
-        const uint32_t idesc = umma::idesc_bf16(BN);
+        const uint32_t idesc = umma::idesc_bf16(NH);
         auto issue = [&](int kt) {
             const int st = kt % NTC_STAGES, dxi = kt / f.Z, sz = kt % f.Z, kc = dxi * C + sz * 64;
             mbar_expect_tx(&s.full[st], TX);
             tma_load_4d(s.ahi[st], &tm_hi, 0, bx0 + dxi - 1, by0 + dyi - 1, sz, &s.full[st]);
             tma_load_4d(s.alo[st], &tm_lo, 0, bx0 + dxi - 1, by0 + dyi - 1, sz, &s.full[st]);
-            tma_load_2d(s.bhi[st], &tm_T, kc, dyi * C, &s.full[st]);
-            tma_load_2d(s.blo[st], &tm_T, K3 + kc, dyi * C, &s.full[st]);
+            tma_load_2d(s.bhi[st], &tm_T, kc, dyi * C + t0, &s.full[st]);
+            tma_load_2d(s.blo[st], &tm_T, K3 + kc, dyi * C + t0, &s.full[st]);
         };
         bool ok = true;
         int issued = 0, landed = 0;
@@ -1477,13 +1478,13 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
         const int bx = bx0 + lane, by = by0 + warp;
         const bool okb = bx < nbx && by < nby;
         const bool vec = (f.X & 3) == 0 && bx * 8 + 8 <= f.X;
-        for (int c0 = 0; c0 < BN; c0 += 16) {
+        for (int c0 = 0; c0 < NH; c0 += 16) {
             float v[16];
             umma::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
             if (!okb) continue;
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int t = c0 + 8 * h, tz = t >> 6, y = by * 8 + ((t >> 3) & 7);
+                const int t = t0 + c0 + 8 * h, tz = t >> 6, y = by * 8 + ((t >> 3) & 7);
                 if (y >= f.Y) continue;
                 float *o = out + ((long long)tz * f.Y + y) * f.X + bx * 8;
                 if (vec) {
@@ -2202,7 +2203,7 @@ int fmm_plan_create(mms_ctx *ctx)
             const cuuint32_t bR[4] = {64, NTC_TW, NTC_TH, 1};
             const cuuint64_t dT[2] = {(cuuint64_t)6 * C, (cuuint64_t)3 * C};
             const cuuint64_t sT[1] = {(cuuint64_t)6 * C * 2};
-            const cuuint32_t bT[2] = {64, (cuuint32_t)C};
+            const cuuint32_t bT[2] = {64, (cuuint32_t)C / 2};
             int e = ntc_tensor_map(&pl->ntc_map[0], pl->ntcR, 4, dR, sR, bR);
             if (e == MMS_OK) e = ntc_tensor_map(&pl->ntc_map[1], pl->ntcR + nR / 2, 4, dR, sR, bR);
             if (e == MMS_OK) e = ntc_tensor_map(&pl->ntc_map[2], pl->ntcT, 2, dT, sT, bT);
@@ -2304,7 +2305,7 @@ static int near_launch(mms_ctx *ctx, const float *rho, cudaStream_t st)
         MMS_CUDA_TRY(launch_k(k_rho_split, dim3((unsigned)div_up(nR, 256)), dim3(256), 0, st, rho, rhi, rlo, f, nbx,
                               nby));
     pl->split_of = nullptr;
-    const dim3 grid((unsigned)(div_up(nbx, NTC_TW) * div_up(nby, NTC_TH)), 3);
+    const dim3 grid((unsigned)(div_up(nbx, NTC_TW) * div_up(nby, NTC_TH)), 3, 2);
 #define X(BN_)                                                                                                  \
     if (64 * f.Z == BN_) {                                                                                      \
         MMS_CUDA_TRY(launch_k(k_p2p_tc<BN_>, grid, dim3(128), ntc_smem<BN_>(), st, pl->ntc_map[0], pl->ntc_map[1], \
