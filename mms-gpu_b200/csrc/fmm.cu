@@ -242,7 +242,8 @@ __device__ __forceinline__ void p2m_item(const float *__restrict__ rho, const fl
 }
 
 __device__ __forceinline__ void m2m_reduce(float *__restrict__ Mall, const float *Ts, const float *Mc, float *red,
-                                           long long off_p, int box, const FmmDev &f, int t, int KT, bool valid);
+                                           long long off_p, int box, const FmmDev &f, int t, int KT, bool valid,
+                                           float *keep = nullptr);
 
 // P2M: CTA = one item, PB leaf boxes of one row (up == 0) or of two rows
 // (up != 0, NR <= 32), thread per (row, box, coefficient).  The charges are
@@ -328,7 +329,8 @@ __device__ __forceinline__ int blk_base(int c, int NE, int NO, int blk)
 // memory; Mc (4 NR: the children's expansions, child c = (cy & 1) 2 +
 // (cx & 1)) and red (4 KT) are the group's shared scratch
 __device__ __forceinline__ void m2m_reduce(float *__restrict__ Mall, const float *Ts, const float *Mc, float *red,
-                                           long long off_p, int box, const FmmDev &f, int t, int KT, bool valid)
+                                           long long off_p, int box, const FmmDev &f, int t, int KT, bool valid,
+                                           float *keep)
 {
     const int NE = f.NE, NO = f.NR - f.NE;
     const int c = t / KT, k = t % KT;
@@ -342,8 +344,11 @@ __device__ __forceinline__ void m2m_reduce(float *__restrict__ Mall, const float
     }
     red[c * KT + k] = acc;
     __syncthreads();
-    if (valid && c == 0 && k < f.NR)
-        Mall[(off_p + box) * f.NR + k] = (red[k] + red[KT + k]) + (red[2 * KT + k] + red[3 * KT + k]);
+    if (valid && c == 0 && k < f.NR) {
+        const float v = (red[k] + red[KT + k]) + (red[2 * KT + k] + red[3 * KT + k]);
+        Mall[(off_p + box) * f.NR + k] = v;
+        if (keep) keep[k] = v;  // (the caller's shared copy for the next level up)
+    }
     __syncthreads();
 }
 
@@ -643,9 +648,10 @@ __device__ __forceinline__ void l2l_top_box(float *__restrict__ Lfin, const floa
 
 // The two top levels in one launch each way (NR <= 32).  CTA = one level-2
 // box.  Upward: its four level-3 children (one 4 KT-thread group each, from
-// their level-4 children), then the box itself from those four.  Downward:
-// the box's local from its M2L partials, then its four level-3 children.  The
-// same item code as the per-level kernels, so the same bits.
+// their level-4 children, which are staged with the operators in one wave of
+// asynchronous copies), then the box itself from those four, kept in shared
+// memory.  Downward: the box's local from its M2L partials, then its four
+// level-3 children.  The arithmetic of the per-level kernels, so the same bits.
 __global__ void __launch_bounds__(512) k_top_m2m(float *__restrict__ Mall, const float *__restrict__ Tb,
                                                  long long off2, long long off3, long long off4, FmmDev f)
 {
@@ -655,14 +661,21 @@ __global__ void __launch_bounds__(512) k_top_m2m(float *__restrict__ Mall, const
     const int tsz = 4 * (NE * NE + NO * NO);
     const int KT = blockDim.x / 16;
     float *Ts = smb;
-    stage_async(Ts, Tb, tsz);
-    __syncthreads();
     const int grp = threadIdx.x / (4 * KT), t = threadIdx.x % (4 * KT);
     float *Mc = Ts + tsz + grp * (4 * f.NR + 4 * KT), *red = Mc + 4 * f.NR;
+    float *G = Ts + tsz + 4 * (4 * f.NR + 4 * KT);  // [4][NR]: the level-3 children, child index = grp
     const int P = blockIdx.x;
     const int cx = 2 * (P % 4) + (grp & 1), cy = 2 * (P / 4) + (grp >> 1);
-    m2m_item(Mall, Ts, Mc, red, off3, off4, 8, cy * 8 + cx, f, t, KT, true);
-    m2m_item(Mall, Ts, Mc, red, off2, off3, 4, P, f, t, KT, grp == 0);
+    for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4) umma::cp_async16(umma::smem_u32(Ts + i), Tb + i, true);
+    for (int i = t; i < 4 * f.NR; i += 4 * KT) {  // the group's four level-4 children
+        const int c = i / f.NR, j = i % f.NR;
+        cp_async4(Mc + i, Mall + (off4 + (long long)(2 * cy + (c >> 1)) * 16 + 2 * cx + (c & 1)) * f.NR + j, true);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    m2m_reduce(Mall, Ts, Mc, red, off3, cy * 8 + cx, f, t, KT, true, G + grp * f.NR);
+    m2m_reduce(Mall, Ts, G, red, off2, P, f, t, KT, grp == 0);
 }
 
 __global__ void __launch_bounds__(128) k_top_l2l(float *__restrict__ Lfin, const float *__restrict__ Lpart,
@@ -2374,7 +2387,8 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
         }
         if (top) {
             MMS_CUDA_TRY(launch_k(k_top_m2m, dim3(16), dim3(16 * KT),
-                                  (tsz + 4 * (4 * (size_t)f.NR + 4 * (size_t)KT)) * sizeof(float), ctx->stream,
+                                  (tsz + 4 * (4 * (size_t)f.NR + 4 * (size_t)KT) + 4 * (size_t)f.NR) * sizeof(float),
+                                  ctx->stream,
                                   pl->Mall, (const float *)pl->Tm2m, pl->lev_off[2], pl->lev_off[3], pl->lev_off[4],
                                   f));
             MMS_LAUNCH_CHECK(ctx);
