@@ -70,3 +70,30 @@ def test_reference_signatures_exported(built):
     ]
     for w in want:
         assert w in demangled, w
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """the ctypes mirrors of the header's structs have the C compiler's size
+    and field offsets (a field added in place of a reserved slot, such as
+    mms_solver.near_mode, must not move the others)"""
+    import mmsb200
+    from mmsb200.ensemble import EnsInstance
+    mirrors = {"mms_grid": mmsb200.Grid, "mms_params": mmsb200.Params, "mms_solver": mmsb200.Solver,
+               "mms_controller": mmsb200.Controller, "mms_record": mmsb200.Record,
+               "mms_ens_instance": EnsInstance}
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "mms_b200.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                 check=True).stdout.splitlines())
+    for cname, py in mirrors.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, f"{cname}.{fname}"
