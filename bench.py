@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--leaf", type=int, default=8, help="FMM leaf side in cells (0 = the library's default)")
     ap.add_argument("--m2l", type=int, default=int(os.environ.get("MMS_BENCH_M2L", "0")),
                     help="FMM M2L: 0 auto, 1 FP32 SIMT, 2 tensor cores (split BF16)")
+    ap.add_argument("--near", type=int, default=0,
+                    help="FMM near field: 0 auto (tensor cores at leaf 8), 1 FP32 k_p2p, 2 tensor cores")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--dt", type=float, default=1e-13)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -235,7 +237,7 @@ def run_ours(args):
     grid = mmsb200.Grid(X, Y, Z, *d)
     params = mmsb200.make_params(external=True, hext_t=hext_t, hext_b=hext_b)
     kind = mmsb200.SOLVER_FMM if args.solver == "fmm" else mmsb200.SOLVER_DIRECT
-    solver = mmsb200.make_solver(kind, args.order, args.leaf, args.m2l)
+    solver = mmsb200.make_solver(kind, args.order, args.leaf, args.m2l, mmsb200.FAR_STAGES, args.near)
     tuned = None
     if kind == mmsb200.SOLVER_FMM and args.order == 0:
         # autotuned: fastest (P, leaf, M2L kernel) within half the metric's 1e-3 target
@@ -373,6 +375,7 @@ def run_ours(args):
         except Exception as e:  # the baseline is reported, never required
             base = {"value": None, "error": str(e)[:200]}
 
+    kern = mmsb200.fmm_stats(ctx) if args.solver == "fmm" else None
     ctx.close()
     if ws > 1:
         import torch.distributed as dist
@@ -387,7 +390,10 @@ def run_ours(args):
            "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"}
     if args.solver == "fmm":
         cfg.update({"P": args.order, "leaf": args.leaf or "auto", "autotune": tuned,
-                    "m2l": {0: "auto", 1: "fp32 simt", 2: "tensor cores (split bf16)"}[args.m2l]})
+                    "m2l": {0: "auto", 1: "fp32 simt", 2: "tensor cores (split bf16)"}[args.m2l],
+                    "near": {0: "auto", 1: "fp32 simt", 2: "tensor cores (split bf16)"}[args.near],
+                    "kernels": {"near": "k_p2p_tc (tcgen05, split bf16)" if kern["near_tc"] else "k_p2p (fp32)",
+                                "m2l": "k_m2l_gemm (tcgen05, split bf16)" if kern["m2l_tc"] else "fp32"}})
     line = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": cfg,
