@@ -11,6 +11,9 @@ ASCII field files, and checkpoints of the FP64 state.
   reference's text layouts (helper_functions.cpp:55-123): for each layer z
   and column x, the y values in order, "%g" formatted.  This is MATLAB's
   column-major order.  FP32 input gives the reference's text exactly.
+  ``save_dynamics`` writes mms_march's records as the reference's
+  dynamics.dat, ``save_npy`` a binary field, and ``AsyncWriter`` runs any of
+  them on a background thread, after the device-to-host copy it waits for.
 * ``save_checkpoint``, ``load_checkpoint`` and ``resume`` keep and restore
   everything a run needs: the FP64 state, its time, the mask, the grid, the
   material and field parameters, the solver and, when bound, the surrogate
@@ -75,6 +78,94 @@ def save_vector3d(path, field):
     (helper_functions.cpp:80-100)"""
     with open(path, "w") as fh:
         append_vector3d(fh, field)
+
+
+def save_npy(path, field):
+    """a field as binary .npy (exact values, any dtype)"""
+    np.save(path, np.asarray(field))
+
+
+def format_record(r):
+    """one line of the reference's dynamics.dat (ode_functions.cpp:330-333):
+    tindex, t, dt, E (eV), Mx, My, Mz, |M|, torque; each value rounded to FP32
+    first, as the reference prints its fptype fields"""
+    vals = (r.t, r.dt, r.E_eV, r.Mx, r.My, r.Mz, r.Mmag, r.torque)
+    return "%d, " % r.tindex + ", ".join(_g(float(np.float32(v))) for v in vals) + " \n"
+
+
+def save_dynamics(path, records):
+    """the records of mms_march (Context.march) as dynamics.dat"""
+    with open(path, "w") as fh:
+        for r in records:
+            fh.write(format_record(r))
+
+
+class AsyncWriter:
+    """Writes fields on a background thread, in submission order, while the
+    caller's GPU work goes on.  ``submit(writer, path, array, event)`` queues
+    ``writer(path, array)`` (save_scalar3d, save_vector3d or save_npy); when
+    ``event`` is given (anything with ``synchronize()``, e.g. a torch CUDA
+    event recorded after a non-blocking device-to-host copy into a pinned
+    buffer), the thread waits for it first.  The array must stay untouched
+    until ``pending()`` is 0 or ``flush()`` returns; ``flush()`` re-raises the
+    first write error."""
+
+    def __init__(self):
+        import queue
+        import threading
+        self._q = queue.Queue()
+        self._err = None
+        self._n = 0
+        self._lock = threading.Lock()
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        while True:
+            job = self._q.get()
+            if job is None:
+                self._q.task_done()
+                return
+            writer, path, array, event = job
+            try:
+                if event is not None:
+                    event.synchronize()
+                writer(path, array)
+            except Exception as e:  # reported by flush()
+                with self._lock:
+                    if self._err is None:
+                        self._err = e
+            finally:
+                with self._lock:
+                    self._n -= 1
+                self._q.task_done()
+
+    def submit(self, writer, path, array, event=None):
+        with self._lock:
+            self._n += 1
+        self._q.put((writer, path, array, event))
+
+    def pending(self):
+        with self._lock:
+            return self._n
+
+    def flush(self):
+        self._q.join()
+        with self._lock:
+            err, self._err = self._err, None
+        if err is not None:
+            raise err
+
+    def close(self):
+        self.flush()
+        self._q.put(None)
+        self._t.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 # ------------------------------------------------------------- checkpoints

@@ -93,3 +93,42 @@ def test_checkpoint_round_trip(tmp_path):
     for k in ("kind", "fmm_order", "fmm_leaf", "m2l_mode", "far_mode", "near_mode"):
         assert getattr(c["solver"], k) == getattr(solver, k)
     assert np.array_equal(c["surrogate_weights"], w)
+
+
+def test_dynamics_record_line():
+    r = mmsb200.Record(7, 1.5e-12, 1e-13, -1234.56789, 0.1, -0.2, 0.97, 8.6e5, 3.3e-7)
+    assert mio.format_record(r) == "7, 1.5e-12, 1e-13, -1234.57, 0.1, -0.2, 0.97, 860000, 3.3e-07 \n"
+
+
+class _Event:
+    def __init__(self):
+        self.waited = 0
+
+    def synchronize(self):
+        self.waited += 1
+
+
+def test_async_writer_matches_the_synchronous_writers(tmp_path):
+    rng = np.random.default_rng(5)
+    s = rng.standard_normal((2, 3, 4)).astype(np.float32)
+    v = rng.standard_normal((2, 3, 4, 3)).astype(np.float32)
+    ev = _Event()
+    with mio.AsyncWriter() as w:
+        w.submit(mio.save_scalar3d, tmp_path / "s_async.dat", s, ev)
+        w.submit(mio.save_vector3d, tmp_path / "v_async.dat", v)
+        w.submit(mio.save_npy, tmp_path / "v.npy", v, ev)
+        w.flush()
+        assert w.pending() == 0 and ev.waited == 2
+    mio.save_scalar3d(tmp_path / "s.dat", s)
+    mio.save_vector3d(tmp_path / "v.dat", v)
+    assert open(tmp_path / "s_async.dat").read() == open(tmp_path / "s.dat").read()
+    assert open(tmp_path / "v_async.dat").read() == open(tmp_path / "v.dat").read()
+    assert np.array_equal(np.load(tmp_path / "v.npy"), v)
+
+
+def test_async_writer_reports_a_failed_write(tmp_path):
+    w = mio.AsyncWriter()
+    w.submit(mio.save_npy, tmp_path / "missing_dir" / "x.npy", np.zeros(3))
+    with pytest.raises(OSError):
+        w.flush()
+    w.close()
