@@ -1296,14 +1296,14 @@ __global__ void k_m2l_gather(const float *__restrict__ Mall, __nv_bfloat16 *__re
 //   phi_(dx,dy)[box][t] = sum_s R[box + (dx, dy)][s] T_(dx,dy)[t][s].
 // Both operands are split into BF16 hi + lo and the tensor cores add
 // R_hi T_hi + R_lo T_hi + R_hi T_lo in FP32 (relative error ~2^-16 per
-// product).  CTA = 4 x 32 boxes x one source box row dy: M = 128 boxes, N = C
-// target cells (<= 256), K = 3 C in steps of one (dx, source layer); each operand
-// tile is one TMA copy in the 128-byte-swizzled layout the MMA reads: the
-// charges from box-major BF16 hi / lo copies of rho (one leaf box layer = one
-// 128-byte row), the operator rows from T.  The three source box rows'
-// partials go to separate buffers that L2P adds in a fixed order.  Few CTAs
-// (three per 128 boxes), so the far-field chain that runs beside it keeps
-// most SMs.
+// product).  CTA = 4 x 32 boxes x one source box row dy x half of the target
+// cells: M = 128 boxes, N = C / 2 target cells (<= 128), K = 3 C in steps of
+// one (dx, source layer); each operand tile is one TMA copy in the
+// 128-byte-swizzled layout the MMA reads: the charges from box-major BF16
+// hi / lo copies of rho (one leaf box layer = one 128-byte row), the operator
+// rows from T.  The three source box rows' partials go to separate buffers
+// that L2P adds in a fixed order.  Few CTAs (six per 128 boxes), so the
+// far-field chain that runs beside it keeps most SMs.
 constexpr int NTC_STAGES = 3;
 
 // BN = C target cells of a box; a CTA takes half of them (N = BN / 2)
@@ -2181,8 +2181,9 @@ int fmm_plan_create(mms_ctx *ctx)
     // near field on the tensor cores (k_p2p_tc) at leaf side 8 with a far field
     // and Z <= 4, by default (near_mode 0) or on request (2); FP32 k_p2p
     // otherwise.  At 256 x 256 x 3 (P = 4) it took the RK4 step from 224 to
-    // 191 us: its 24 CTAs leave the SMs' FMA and load pipes to the far-field
-    // chain that runs beside it, where k_p2p's 256 CTAs competed with it.
+    // 191 us (174 us with the later changes): its few CTAs (24, now 48) leave
+    // the SMs' FMA and load pipes to the far-field chain that runs beside it,
+    // where k_p2p's 256 CTAs competed with it.
     const int nmode = ctx->s.near_mode;
     const bool ntc_ok = s == 8 && leaf_threads(f) > 0 && f.L >= 2 && Z <= 4;
     if (nmode < 0 || nmode > 2 || (nmode == 2 && !ntc_ok)) {
