@@ -1328,7 +1328,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
                  : "memory");
 }
 
-// TMA tile loads into shared memory (no multicast), completing on an mbarrier
+// TMA tile loads into this CTA's shared memory, completing on an mbarrier
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int c0, int c1, uint64_t *bar)
 {
     asm volatile(

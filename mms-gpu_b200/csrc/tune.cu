@@ -1,6 +1,6 @@
 // Autotuner: picks the FMM expansion order, leaf side and M2L kernel for a
 // grid by measurement.  Every candidate evaluates the potential of a sample
-// charge density; its error is judged against the exact direct sum computed
+// charge density; its error is measured against the exact direct sum computed
 // on the same device (FP32 table + compensated sums, within 2e-6 of FP64),
 // and the fastest candidate within the error target wins.  Results are cached
 // in-process per shape class (grid dims, cell size, target).

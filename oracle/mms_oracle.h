@@ -2,7 +2,7 @@
  * Test infrastructure only: the CPU oracle for the demag / LLG hot path.
  *
  * A plain-C restatement of the reference's per-step arithmetic, in FP64 (the
- * ground truth every GPU result is judged against) and, where the reference's
+ * ground truth every GPU result is checked against) and, where the reference's
  * own FP32 operation order matters for a tight pin, in FP32.  Only tests/,
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it; the
  * product library never does.
