@@ -243,8 +243,11 @@ int mms_ens_sync(mms_ens *ens);
  * limited to xdim*ydim*zdim <= 1,048,576 cells and xdim <= 2048 (MMS_ERR_ARG
  * beyond).  rho/phi are device arrays; the work is queued on `stream` (a
  * cudaStream_t, NULL = legacy default stream).  The first call on each device
- * performs a one-time set-up (the table's device address, a kernel attribute)
- * with that device current; make that first call before any stream capture.
+ * performs a one-time set-up (it looks up the table's device address) with
+ * that device current; make that first call before any stream capture.  Every
+ * call also raises the sum kernel's shared-memory limit when its row length
+ * needs it (a host-side attribute, no allocation).  A CUDA error left pending
+ * by earlier work is reported as such (MMS_ERR_CUDA) before anything is queued.
  * All calls share the one table, which keeps the last call's contents: calls
  * that overlap on the GPU (different streams, or different host threads on one
  * device) race and must be serialised by the caller. */

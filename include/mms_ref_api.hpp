@@ -3,7 +3,7 @@
  * fptype = float, Vector3 = three packed floats), implemented on top of the C
  * ABI in mms_b200.h.  Linking libmms_refapi.so in place of the reference's
  * fmm_kernel.o + ode_functions.o lets the reference's main.cpp driver run its
- * whole demag / LLG path on the B200 unchanged (see INTEGRATION.md).
+ * whole demag / LLG path on the B200 unchanged.
  *
  *   fmm_calc                   helper_functions.hpp:24-29   (fmm_calc.cu:295-408)
  *   calc_potential_exact       helper_functions.hpp:31-35   (fmm_calc.cu:412-461)

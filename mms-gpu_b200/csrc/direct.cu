@@ -27,6 +27,8 @@
 
 #include <math.h>
 
+#include <mutex>
+
 namespace {
 
 constexpr int TX = 8;            // targets per lane
@@ -201,9 +203,12 @@ int direct_build_table(mms_ctx *ctx)
     if (!ctx->gtab) MMS_TRY(ctx_alloc(ctx, &ctx->gtab, (size_t)ctx->N));
     k_build_gtab<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->gtab, ctx->gk());
     MMS_LAUNCH_CHECK(ctx);
-    const size_t smem = direct_smem_bytes(ctx->g.xdim);
-    if (smem > 48 * 1024)
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // The attribute is per kernel, shared by every context and by the
+    // allocation-free entry point: always raise it to the widest supported
+    // row, so that no caller ever lowers it below another caller's need.
+    if (direct_smem_bytes(ctx->g.xdim) > 48 * 1024)
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)direct_smem_bytes(MAX_X)));
     return MMS_OK;
 }
 
@@ -236,6 +241,8 @@ static __device__ __align__(256) float g_noalloc_gtab[MMS_NOALLOC_MAX_CELLS];
 namespace {
 constexpr int NOALLOC_MAX_DEVICES = 64;
 float *g_noalloc_ptr[NOALLOC_MAX_DEVICES];   // device address of g_noalloc_gtab, per device
+std::once_flag g_noalloc_once[NOALLOC_MAX_DEVICES];
+cudaError_t g_noalloc_setup_err[NOALLOC_MAX_DEVICES];
 }  // namespace
 
 extern "C" int mms_potential_direct_noalloc(const float *rho, float *phi, int xdim, int ydim, int zdim, double dx,
@@ -257,14 +264,36 @@ extern "C" int mms_potential_direct_noalloc(const float *rho, float *phi, int xd
         mms_set_error("mms_potential_direct_noalloc: device %d out of range", dev);
         return MMS_ERR_ARG;
     }
-    if (!g_noalloc_ptr[dev]) {
-        // one-time set-up on this device (the first call, with the device current)
+    // An error left pending by the caller's earlier work is not this call's:
+    // report it as such instead of blaming the launches below.
+    {
+        const cudaError_t pend = cudaPeekAtLastError();
+        if (pend != cudaSuccess) {
+            mms_set_error("mms_potential_direct_noalloc: a CUDA error was pending before the call: %s",
+                          cudaGetErrorString(pend));
+            return MMS_ERR_CUDA;
+        }
+    }
+    // one-time set-up on this device (the first call, with the device
+    // current): the table's device address.  Host threads racing on the
+    // first call run it once.
+    std::call_once(g_noalloc_once[dev], [dev]() {
         float *p = nullptr;
-        MMS_CUDA_TRY(cudaGetSymbolAddress((void **)&p, g_noalloc_gtab));
+        g_noalloc_setup_err[dev] = cudaGetSymbolAddress((void **)&p, g_noalloc_gtab);
+        if (g_noalloc_setup_err[dev] == cudaSuccess) g_noalloc_ptr[dev] = p;
+    });
+    if (g_noalloc_setup_err[dev] != cudaSuccess || !g_noalloc_ptr[dev]) {
+        mms_set_error("mms_potential_direct_noalloc: cudaGetSymbolAddress: %s",
+                      cudaGetErrorString(g_noalloc_setup_err[dev]));
+        return MMS_ERR_CUDA;
+    }
+    // The kernel's shared-memory limit is a per-kernel attribute that a
+    // context may also set; set it on every call (host-side, allocates
+    // nothing) so that it always covers this call's row length.
+    const size_t smem = direct_smem_bytes(xdim);
+    if (smem > 48 * 1024)
         MMS_CUDA_TRY(cudaFuncSetAttribute(k_direct, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)direct_smem_bytes(MAX_X)));
-        g_noalloc_ptr[dev] = p;
-    }
     float *gtab = g_noalloc_ptr[dev];
     GridK g;
     g.X = xdim;
@@ -279,7 +308,7 @@ extern "C" int mms_potential_direct_noalloc(const float *rho, float *phi, int xd
     k_build_gtab<<<div_up(N, 256), 256, 0, st>>>(gtab, g);
     MMS_CUDA_TRY(cudaGetLastError());
     dim3 grid((unsigned)(ydim * zdim), div_up(xdim, SEG));
-    k_direct<<<grid, DWARPS * 32, direct_smem_bytes(xdim), st>>>(rho, gtab, phi, g);
+    k_direct<<<grid, DWARPS * 32, smem, st>>>(rho, gtab, phi, g);
     MMS_CUDA_TRY(cudaGetLastError());
     return MMS_OK;
 }

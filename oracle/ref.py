@@ -132,3 +132,26 @@ def time_hfield(M, dims, d, use_fmm=False, P=3, reps=1, threads=None):
         out = _run("time_hfield", kw, env=env)
         s, th = out.split()
         return float(s), int(th)
+
+
+def time_rk4(material, M, dims, d, dt, nsteps, warmup=0, use_fmm=False, P=3, threads=None, budget_s=None):
+    """Wall seconds of each of `nsteps` real reference RK4 steps (rk4_step +
+    the post-step Hfield, time_marching's accepted-step order) after `warmup`
+    untimed ones.  Returns (per-step seconds, threads); fewer steps than asked
+    when `budget_s` seconds of timed work ran out."""
+    env = {"OMP_NUM_THREADS": str(threads)} if threads else None
+    with tempfile.TemporaryDirectory() as td:
+        np.ascontiguousarray(material, np.uint8).tofile(os.path.join(td, "mat"))
+        np.ascontiguousarray(M, np.float32).tofile(os.path.join(td, "M"))
+        kw = _grid_kw(dims, d)
+        kw.update(material=os.path.join(td, "mat"), M=os.path.join(td, "M"), dt=repr(float(dt)), nsteps=nsteps,
+                  warmup=warmup, use_fmm=int(use_fmm), P=P)
+        if budget_s is not None:
+            kw["budget_s"] = repr(float(budget_s))
+        out = _run("time_rk4", kw, env=env)
+        lines = out.strip().splitlines()
+        tot = lines[-1].split()
+        assert tot[0] == "total", out[-200:]
+        steps = [float(v) for v in lines[:-1]]
+        assert len(steps) == int(tot[1])
+        return steps, int(tot[3])

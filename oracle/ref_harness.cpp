@@ -103,7 +103,7 @@ static double now_s()
 int main(int argc, char **argv)
 {
     if (argc < 2) {
-        fprintf(stderr, "usage: mmsref_harness <potential|hfield|stencils|rk4|march|time_hfield> key=value...\n");
+        fprintf(stderr, "usage: mmsref_harness <potential|hfield|stencils|rk4|march|time_rk4|time_hfield> key=value...\n");
         return 2;
     }
     const std::string op = argv[1];
@@ -203,6 +203,53 @@ int main(int argc, char **argv)
                                xdim, ydim, zdim, dx, dy, dz, P, mu_0, Ms, Aexch, alfa, gamma,
                                demag, exchange, external, use_fmm, 0, sim, verbosity);
         write_bin(out + ".M", M.data(), N);
+        return st ? 1 : 0;
+    }
+    if (op == "time_rk4") {
+        /* CPU baseline: `warmup` untimed then `nsteps` timed fixed-dt steps in
+         * time_marching's accepted-step order (ode_functions.cpp:230-308): per
+         * step rk4_step at t (three Hfield calls inside, :109-133) then
+         * Hfield(M2) at the old t (:267).  The initial Hfield(M) is untimed.
+         * Stops early, after the step that passes `budget_s` seconds of timed
+         * work.  Prints one line per timed step (its wall seconds), then
+         * "total <steps> <seconds> <threads>". */
+        std::vector<byte> material = read_bin<byte>(arg_s("material"), N);
+        std::vector<Vector3> M = read_bin<Vector3>(arg_s("M"), N);
+        std::vector<Vector3> M2(N), H(N), H2(N), H3(N), slope(N), this_slope(N);
+        std::vector<fptype> charge(N), pot(N);
+        const fptype dt = arg_f("dt");
+        const int nsteps = arg_i("nsteps"), warmup = arg_i("warmup", 0);
+        const double budget = arg_f("budget_s", 1e30);
+        fptype t = 0, t2 = 0;
+        int st = Hfield(M.data(), H.data(), charge.data(), pot.data(), t, xdim, ydim, zdim, dx, dy, dz, P,
+                        mu_0, Ms, Aexch, demag, exchange, external, use_fmm, 0, verbosity);
+        double timed = 0;
+        int done = 0;
+        for (int s = 0; s < warmup + nsteps && !st; s++) {
+            const double t0 = now_s();
+            H3 = H;
+            st |= rk4_step(t, dt, &t2, material.data(), M.data(), M2.data(), H3.data(), slope.data(),
+                           this_slope.data(), charge.data(), pot.data(), xdim, ydim, zdim, dx, dy, dz, P,
+                           mu_0, Ms, Aexch, alfa, gamma, demag, exchange, external, use_fmm, 1, 0, verbosity);
+            st |= Hfield(M2.data(), H2.data(), charge.data(), pot.data(), t, xdim, ydim, zdim, dx, dy, dz, P,
+                         mu_0, Ms, Aexch, demag, exchange, external, use_fmm, 0, verbosity);
+            M.swap(M2);
+            H.swap(H2);
+            t = t2;
+            const double t1 = now_s();
+            if (s >= warmup) {
+                printf("%.9f\n", t1 - t0);
+                timed += t1 - t0;
+                done++;
+                if (timed > budget) break;
+            }
+        }
+        int threads = 1;
+#ifdef _OPENMP
+        threads = omp_get_max_threads();
+#endif
+        printf("total %d %.9f %d\n", done, timed, threads);
+        if (!out.empty()) write_bin(out + ".M", M.data(), N);
         return st ? 1 : 0;
     }
     if (op == "time_hfield") {

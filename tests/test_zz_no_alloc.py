@@ -8,8 +8,10 @@ inside the library.  This file checks, through the C ABI, that it returns what
 the context-based entry point (mms_potential_dev with the direct solver)
 returns, within the direct sum's tolerance (rel-L2 <= 2e-6), on two calls in a
 row with different grids, that it allocates nothing, and that sizes beyond its
-fixed table are refused.  It runs last (file name) and passes alone or after
-the other tests.
+fixed table are refused.  A wide-row case checks both entry points against the
+FP64 oracle after a context of another row length has set the sum kernel's
+shared-memory limit (the limit is per kernel, shared by both entry points).
+It runs last (file name) and passes alone or after the other tests.
 """
 import ctypes
 
@@ -65,3 +67,33 @@ def test_noalloc_rejects_sizes_beyond_its_table(cuda, lib):
     st = _noalloc(lib, rho, phi, (1024, 1024, 2), (5e-9, 5e-9, 5e-9), 0)
     assert st == mmsb200.MMS_ERR_ARG
     assert b"exceeds" in lib.mms_last_error()
+
+
+def test_noalloc_wide_rows_after_a_context_of_another_width(cuda, lib, oracle_mod):
+    """A context whose rows need more than 48 KB of shared memory (xdim 900)
+    sets the sum kernel's limit; an allocation-free call with wider rows
+    (xdim 1100) must still launch, and both results must match the FP64 sum."""
+    import mmsb200
+    torch = cuda
+    stream = torch.cuda.current_stream().cuda_stream
+    d = (5e-9, 5e-9, 5e-9)
+    results = []
+    for dims, seed, use_ctx in (((900, 4, 2), 11, True), ((1100, 8, 3), 12, False)):
+        X, Y, Z = dims
+        rng = np.random.default_rng(seed)
+        rho_h = (rng.standard_normal((Z, Y, X)) * 1e14).astype(np.float32)
+        rho = torch.from_numpy(rho_h).cuda()
+        phi = torch.full_like(rho, float("nan"))
+        if use_ctx:
+            with mmsb200.Context(mmsb200.Grid(X, Y, Z, *d), mmsb200.make_params(),
+                                 mmsb200.make_solver(mmsb200.SOLVER_DIRECT), stream=stream) as ctx:
+                ctx.potential_dev(rho, phi)
+                ctx.sync()
+        else:
+            st = _noalloc(lib, rho, phi, dims, d, stream)
+            assert st == mmsb200.MMS_OK, lib.mms_last_error()
+        torch.cuda.synchronize()
+        ref = oracle_mod.potential_direct(oracle_mod.Grid(X, Y, Z, *d), rho_h.astype(np.float64))
+        results.append(rel_l2(phi.cpu().numpy(), ref))
+    assert results[0] <= 2e-6, results
+    assert results[1] <= 2e-6, results
