@@ -54,10 +54,10 @@ typedef enum {
 typedef enum {
     MMS_SOLVER_DIRECT = 0,   /* exact O(N^2) sum, FP32 tiles, compensated      */
     MMS_SOLVER_FMM = 1,      /* spherical-harmonic FMM, exact near field       */
-    MMS_SOLVER_SURROGATE = 2 /* exact near field (FMM P2P, leaf 4) + far field
-                                from the learned operator (mms_sno_*); the FMM
-                                of the same order checks it and takes over
-                                (mms_ctx_set_surrogate)                       */
+    MMS_SOLVER_SURROGATE = 2 /* exact near field (FMM P2P, leaf 8) + far field
+                                from the learned operator (mms_farnet_*); the
+                                FMM of the solver's order checks it and takes
+                                over (mms_ctx_set_surrogate)                  */
 } mms_solver_kind;
 
 typedef struct {
@@ -274,43 +274,55 @@ int mms_autotune_fmm_steps(const mms_grid *grid, const mms_params *params, const
                            mms_solver *best, double *best_ms, double *best_err);
 
 /* surrogate far field ---------------------------------------------------------
- * A 3-D convolutional neural operator (U-Net over the 4 x 4-cell patch grid,
- * 4 levels, 32 channels, BF16 weights, FP32 accumulation, no biases or
- * activations: the map is linear) from the dimensionless cell charge
- * u = rho dx / Ms to the dimensionless far-field potential
- * phi_far / (Ms dx) for cubic cells, where phi_far = phi - (exact near field
- * over the 3 x 3 leaf-box neighbourhood, leaf side 4, all layers).  Forward,
- * backward and the optimiser are the library's own tcgen05 kernels.  No
- * reference counterpart (the reference has no learned component). */
-typedef struct mms_sno mms_sno;
-long long mms_sno_num_params(void);
-/* a network for [batch][zdim][ydim][xdim] cell arrays on the current device */
-int mms_sno_create(int xdim, int ydim, int zdim, int batch, mms_sno **out);
-void mms_sno_destroy(mms_sno *net);
-/* FP32 master weights, host arrays of mms_sno_num_params() values; per layer
- * [cout][tap][cin] in layer order.  get with bf16_rounded != 0 returns the
- * BF16 values the kernels use. */
-int mms_sno_set_weights(mms_sno *net, const float *w, long long count);
-int mms_sno_get_weights(mms_sno *net, float *w, long long count, int bf16_rounded);
-/* out = network(u) for nbatch <= batch samples (device arrays, legacy stream) */
-int mms_sno_forward_dev(mms_sno *net, const float *u, float *out, int nbatch);
-/* loss = mean_b |net(u_b) - far_b|^2 / |far_b|^2 and its gradient w.r.t. the
- * FP32 weights (host array, may be NULL); device inputs */
-int mms_sno_gradient(mms_sno *net, const float *u, const float *far, int nbatch, float *grad, double *loss);
+ * A learned far-field operator for thin films of 3 layers on cubic cells: a
+ * linear multilevel convolutional network over the quadtree of 8 x 8 x 3 leaf
+ * boxes with the FMM's data flow and its own weights per level.  The encoder
+ * (replacing P2M) maps a leaf box's 192 cell charges to 24 channels (16 even,
+ * 8 odd under z -> -z); 2 x 2 stride-2 convolutions go down the tree (M2M);
+ * at every level a parity-aware 7 x 7 convolution over the interaction list
+ * (children of the parent's neighbours that are not neighbours, the
+ * reference's Box.cu:171-195) couples boxes (M2L); transposed convolutions go
+ * back up (L2L) and the decoder (L2P) gives the far field at every cell.  The
+ * near field over each leaf box's 3 x 3 neighbourhood stays exact.  Weights:
+ * FP32, mms_farnet_num_params() of them, indexed by depth below the leaves, so
+ * one vector serves every grid of 2..6 quadtree levels (up to 512 cells a
+ * side); they start from nested SVD bases of the 1/r interactions and are
+ * trained on FMM-generated (charge, far field) pairs by the kernels below.  It
+ * replaces the far-field pass of the reference's fmm_calc (fmm_calc.cu:
+ * 186-222); the reference has no learned component.
+ *
+ * Units: u = rho dx / Ms (dimensionless cell charge) in, phi_far / (Ms dx) out;
+ * arrays are [batch][3][ydim][xdim] FP32 on the device.  All calls below run
+ * on the legacy default stream and return when their results are ready. */
+typedef struct mms_farnet mms_farnet;
+long long mms_farnet_num_params(void);
+/* a network for batches of up to `batch` samples of an xdim x ydim x 3 grid
+ * (17..512 cells a side: 2..6 quadtree levels of 8-cell leaves) */
+int mms_farnet_create(int xdim, int ydim, int batch, mms_farnet **out);
+void mms_farnet_destroy(mms_farnet *net);
+/* host arrays of mms_farnet_num_params() FP32 weights; set also resets Adam */
+int mms_farnet_set_weights(mms_farnet *net, const float *w, long long count);
+int mms_farnet_get_weights(mms_farnet *net, float *w, long long count);
+/* out = far field of u for nbatch <= batch samples */
+int mms_farnet_forward_dev(mms_farnet *net, const float *u, float *out, int nbatch);
+/* loss = mean_b |net(u_b) - far_b|^2 / nrm2_b (nrm2_b = |phi_b|^2 of the total
+ * potential, so the loss is the squared relative error of phi) and its
+ * gradient with respect to the weights (host array, may be NULL); u, far:
+ * device [nbatch][3][Y][X]; nrm2: device [nbatch] */
+int mms_farnet_gradient(mms_farnet *net, const float *u, const float *far, const float *nrm2, int nbatch,
+                        float *grad, double *loss);
 /* one Adam step on that loss; *loss is the loss before the step */
-int mms_sno_train_step(mms_sno *net, const float *u, const float *far, int nbatch, float lr, float beta1,
-                       float beta2, float eps, double *loss);
-long long mms_sno_device_bytes(const mms_sno *net);
+int mms_farnet_train_step(mms_farnet *net, const float *u, const float *far, const float *nrm2, int nbatch,
+                          float lr, float beta1, float beta2, float eps, double *loss);
+long long mms_farnet_device_bytes(const mms_farnet *net);
 
-/* Binds trained weights to a context whose solver is MMS_SOLVER_SURROGATE and
- * arms its check: every `check_every` steps (0: never) of mms_run_fixed, and
- * every `check_every` accepted steps plus every rejected step of mms_march,
- * the potential of the current state is computed by both the surrogate and
- * the FMM (the solver's order, leaf 4); when their rel-L2 difference exceeds
- * `tol` the FMM replaces the surrogate for the rest of the run.  fast != 0:
- * the network runs on BF16 activations (hi products only: half the tensor-core
- * work, ~1e-3 relative rounding of the far field) instead of hi/lo pairs.
- * Cubic cells only. */
+/* Binds trained weights to a context whose solver is MMS_SOLVER_SURROGATE
+ * (leaf side 8, zdim 3, cubic cells) and arms its check: every `check_every`
+ * steps (0: never) of mms_run_fixed, and every `check_every` accepted steps
+ * plus every rejected step of mms_march, the potential of the current state
+ * is computed by both the network and the FMM (the solver's order P, leaf 8);
+ * when their rel-L2 difference exceeds `tol` the FMM replaces the network for
+ * the rest of the run.  `fast` is reserved and must be 0. */
 int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol, int fast);
 /* runs that check now on the current state; *err = rel-L2(surrogate, FMM) */
 int mms_surrogate_check(mms_ctx *ctx, double *err);
@@ -327,7 +339,8 @@ int mms_potential_split_dev(mms_ctx *ctx, const float *rho, float *phi, float *n
  * or C += A B^T (beta 1); A M x K and B N x K row-major (K contiguous), C
  * M x N FP32 row-major; K, lda, ldb multiples of 8; bn = 64 or 128 (tile N).
  * Device pointers; synchronises `stream`.  No reference counterpart (used to
- * validate the core behind the tensor-core M2L and the surrogate). */
+ * validate the core behind the tensor-core M2L and the network's weight
+ * gradients). */
 int mms_diag_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C, int ldc,
                        int M, int N, int K, int beta, int bn, void *stream);
 /* FP32 FMA throughput of the current device in TFLOP/s (a microbenchmark of

@@ -228,7 +228,6 @@ int surrogate_check_now(mms_ctx *ctx, double *err_out)
     MMS_TRY(launch_potential_fmm(ctx, ctx->rho, pf));
     double err = 0;
     MMS_TRY(rel_l2_dev(ctx, ps, pf, ctx->N, &err));
-    MMS_TRY(sno_error_flag(ctx->sno, ctx->stream));
     ctx->sur_checks++;
     ctx->sur_last_err = err;
     ctx->sur_max_err = std::max(ctx->sur_max_err, err);
@@ -247,7 +246,7 @@ int surrogate_check_now(mms_ctx *ctx, double *err_out)
 
 bool surrogate_armed(const mms_ctx *ctx)
 {
-    return ctx->s.kind == MMS_SOLVER_SURROGATE && ctx->sno && ctx->sur_active && ctx->sur_every > 0;
+    return ctx->s.kind == MMS_SOLVER_SURROGATE && ctx->sur_bound && ctx->sur_active && ctx->sur_every > 0;
 }
 
 int read_stats(mms_ctx *ctx, double out[STAT_SLOTS])
@@ -415,7 +414,6 @@ int mms_ctx_destroy(mms_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     drop_graph(ctx);
     fmm_plan_destroy(ctx);
-    if (ctx->sno) mms_sno_destroy(ctx->sno);
     void *bufs[] = {ctx->rho, ctx->phi, ctx->phibak, ctx->vecA, ctx->vecB, ctx->gtab, ctx->mat, ctx->M, ctx->A,
                     ctx->B, ctx->K, ctx->Mbak, ctx->Mfull, ctx->tstate, ctx->hext, ctx->stat_part, ctx->stats};
     for (void *b : bufs)
@@ -447,6 +445,7 @@ int mms_ctx_set_solver(mms_ctx *ctx, const mms_solver *solver)
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     drop_graph(ctx);
     fmm_plan_destroy(ctx);
+    ctx->sur_bound = false;  // the network's tables lived in the plan
     ctx->s = *solver;
     if (ctx->s.kind == MMS_SOLVER_FMM || ctx->s.kind == MMS_SOLVER_SURROGATE) {
         MMS_TRY(fmm_plan_create(ctx));
@@ -874,13 +873,15 @@ int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int che
         mms_set_error("mms_ctx_set_surrogate: the network is trained for cubic cells");
         return MMS_ERR_ARG;
     }
-    MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    if (!ctx->sno) {
-        MMS_TRY(mms_sno_create(ctx->g.xdim, ctx->g.ydim, ctx->g.zdim, 1, &ctx->sno));
-        ctx->dev_bytes += (size_t)mms_sno_device_bytes(ctx->sno);
+    if (fast != 0) {
+        mms_set_error("mms_ctx_set_surrogate: `fast` is reserved and must be 0");
+        return MMS_ERR_ARG;
     }
-    MMS_TRY(mms_sno_set_weights(ctx->sno, w, count));
-    sno_set_fast(ctx->sno, fast != 0);
+    MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    const size_t before = fmm_plan_bytes(ctx);
+    MMS_TRY(farnet_bind(ctx, w, count));
+    ctx->dev_bytes += fmm_plan_bytes(ctx) - before;
+    ctx->sur_bound = true;
     ctx->sur_every = check_every;
     ctx->sur_tol = tol;
     ctx->sur_active = true;
@@ -894,7 +895,7 @@ int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int che
 int mms_surrogate_check(mms_ctx *ctx, double *err)
 {
     MMS_TRY(require_state(ctx));
-    if (ctx->s.kind != MMS_SOLVER_SURROGATE || !ctx->sno) {
+    if (ctx->s.kind != MMS_SOLVER_SURROGATE || !ctx->sur_bound) {
         mms_set_error("mms_surrogate_check: no surrogate bound to this context");
         return MMS_ERR_ARG;
     }
@@ -908,7 +909,7 @@ int mms_surrogate_stats(const mms_ctx *ctx, int *active, long long *checks, long
         mms_set_error("context is NULL");
         return MMS_ERR_ARG;
     }
-    if (active) *active = ctx->s.kind == MMS_SOLVER_SURROGATE && ctx->sno && ctx->sur_active;
+    if (active) *active = ctx->s.kind == MMS_SOLVER_SURROGATE && ctx->sur_bound && ctx->sur_active;
     if (checks) *checks = ctx->sur_checks;
     if (fallbacks) *fallbacks = ctx->sur_fallbacks;
     if (last_err) *last_err = ctx->sur_last_err;

@@ -30,6 +30,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
+#include "farnet.cuh"
 #include "fmm_ops.hpp"
 #include "mms_internal.cuh"
 #include "umma.cuh"
@@ -111,6 +112,17 @@ struct FmmPlan {
     cudaStream_t side = nullptr;   // P2P runs here, concurrently with P2M .. L2L
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     size_t bytes = 0;
+    // learned far-field network (solver MMS_SOLVER_SURROGATE): tables per
+    // level, bound by farnet_bind from a weight vector indexed by depth
+    int fn_ready = 0;
+    float *fnW = nullptr;     // [NR][C] encoder (transposed), dx^2 folded in
+    float *fnV = nullptr;     // [NR][C] decoder
+    float *fnM2L = nullptr;   // [levels 2..L][49][OSZ]
+    float *fnM2M = nullptr;   // [parent levels 2..L-1][4][OSZ]
+    float *fnL2L = nullptr;   // [parent levels 2..L-1][4][OSZ]
+    float *fnM = nullptr;     // [boxes of all levels][NR] multipoles
+    float *fnLp = nullptr;    // [boxes of all levels][NR] interaction-list locals
+    unsigned *fnCtr = nullptr;  // [boxes] arrival counters of the upward pass (zero between launches)
     // algorithmic work per evaluation (for the roofline)
     double flops = 0;
     double stage_flops[5] = {0, 0, 0, 0, 0};  // P2M, M2M, M2L, L2L, L2P+P2P
@@ -588,15 +600,20 @@ __device__ __forceinline__ void m2l_res_item(const float *__restrict__ Mall, flo
 // fits beside two k_p2p CTAs of 288 threads x 64 registers; the near field
 // runs concurrently with the M2L and, at 117 registers, the M2L's CTAs waited
 // for the near field's to finish.  256 threads per CTA.
+// lstride: floats between the operator tables of consecutive levels (tables
+// of level l at Tc + (l - 2) lstride); 0 when one table serves every level
+// (the spherical-harmonic operators, lengths in box widths).
 template <int NR_, int NE_>
 __global__ void __maxnreg__(NR_ <= 30 ? 112 : 255) k_m2l_res(const float *__restrict__ Mall, float *__restrict__ Lout,
                                                             const float *__restrict__ Tc, const int4 *__restrict__ items,
-                                                            const long long *__restrict__ lev_off, FmmDev f)
+                                                            const long long *__restrict__ lev_off, FmmDev f,
+                                                            long long lstride)
 {
     pdl_begin();
     constexpr int NO_ = NR_ - NE_;
     constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
     extern __shared__ __align__(16) float sr[];
+    Tc += (long long)(items[blockIdx.x].x - 2) * lstride;
     // stage the operator table with asynchronous copies: every 16-byte chunk
     // in flight at once instead of one load-store round trip per chunk
     for (int i = threadIdx.x * 4; i < 49 * OSZ; i += blockDim.x * 4)
@@ -1710,7 +1727,7 @@ int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float
 }
 
 // resident-operator M2L specialisations: (NR, NE) for P = 1 .. 5
-#define MMS_M2L_RES_CASES(X) X(6, 4) X(12, 8) X(20, 12) X(30, 18) X(42, 24)
+#define MMS_M2L_RES_CASES(X) X(6, 4) X(12, 8) X(20, 12) X(24, 16) X(30, 18) X(42, 24)
 
 int m2l_res_supported(int NR, int NE)
 {
@@ -1741,10 +1758,10 @@ int m2l_res_prepare(int NR, int NE)
 }
 
 int m2l_res_launch(const FmmDev &f, int nitems, const float *Mall, float *Lout, const float *Tc, const int4 *items,
-                   const long long *lev, cudaStream_t st)
+                   const long long *lev, cudaStream_t st, long long lstride = 0)
 {
     const size_t sm = m2l_res_smem(f.NR, f.NE);
-#define X(a, c) if (f.NR == a && f.NE == c) { MMS_CUDA_TRY(launch_k(k_m2l_res<a, c>, dim3(nitems), dim3(32 * RES_WARPS), sm, st, Mall, Lout, Tc, items, lev, f)); return MMS_OK; }
+#define X(a, c) if (f.NR == a && f.NE == c) { MMS_CUDA_TRY(launch_k(k_m2l_res<a, c>, dim3(nitems), dim3(32 * RES_WARPS), sm, st, Mall, Lout, Tc, items, lev, f, lstride)); return MMS_OK; }
     MMS_M2L_RES_CASES(X)
 #undef X
     mms_set_error("no resident M2L kernel for NR=%d", f.NR);
@@ -1791,9 +1808,10 @@ int fmm_plan_create(mms_ctx *ctx)
         return MMS_ERR_ARG;
     }
     int s = ctx->s.fmm_leaf;
-    if (s == 0) s = ctx->s.kind == MMS_SOLVER_SURROGATE ? 4 : fmm_default_leaf(P, ctx->g.xdim, ctx->g.ydim);
-    if (ctx->s.kind == MMS_SOLVER_SURROGATE && s != 4) {
-        mms_set_error("the surrogate solver needs leaf side 4 (its patch), got %d", s);
+    if (s == 0) s = ctx->s.kind == MMS_SOLVER_SURROGATE ? FN_S : fmm_default_leaf(P, ctx->g.xdim, ctx->g.ydim);
+    if (ctx->s.kind == MMS_SOLVER_SURROGATE && (s != FN_S || ctx->g.zdim != FN_Z)) {
+        mms_set_error("the surrogate solver works on %d x %d x %d leaf boxes (leaf side %d, %d layers given)", FN_S,
+                      FN_S, FN_Z, s, ctx->g.zdim);
         return MMS_ERR_ARG;
     }
     if (s < 1 || s > 16) {
@@ -2257,7 +2275,8 @@ void fmm_plan_destroy(mms_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     void *b[] = {pl->Wt, pl->Vt, pl->Tm2m, pl->Tl2l, pl->Tm2l, pl->Tm2lc, pl->Gn, pl->Mall, pl->Lall, pl->Lpart,
                  pl->m2l_items, pl->res_items, pl->lev_dev, pl->near, pl->tcA[0], pl->tcA[1], pl->tcB, pl->tc_rowmap,
-                 pl->tc_rowinfo, pl->tc_groups, pl->far_sync, pl->ntcT, pl->ntcR, pl->near3};
+                 pl->tc_rowinfo, pl->tc_groups, pl->far_sync, pl->ntcT, pl->ntcR, pl->near3, pl->fnW, pl->fnV,
+                 pl->fnM2L, pl->fnM2M, pl->fnL2L, pl->fnM, pl->fnLp, pl->fnCtr};
     for (void *p : b)
         if (p) cudaFree(p);
     if (pl->side) cudaStreamSynchronize(pl->side);
@@ -2592,26 +2611,426 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
     return l2p_launch_far(ctx, rho, phi);
 }
 
-// surrogate potential: the exact near field on the side stream, the learned
-// far field on the main one; the network's last layer adds the two
+// ===========================================================================
+// Learned far-field network (solver MMS_SOLVER_SURROGATE).
+//
+// A linear multilevel convolutional operator over the quadtree of 8 x 8 x 3
+// leaf boxes, with the FMM's data flow and its own per-level weights:
+//   encoder  m_leaf = W^T q                      (replaces P2M)
+//   down     m_par  = sum_child M2M_l m_child     (replaces M2M)
+//   lateral  l_t   += sum_{o in IL(t)} M2L_l m_{t-o}  (replaces M2L; the
+//                     reference's interaction lists, Box.cu:171-195)
+//   up       l_chd += L2L_l l_par                (replaces L2L)
+//   decoder  phi    = V^T l_leaf + exact near field (replaces L2P; the near
+//                     field is the FMM's own P2P over the 3 x 3 leaf
+//                     neighbourhood)
+// Widths: FN_NE channels even and FN_NO odd under z -> -z, every table block
+// diagonal (the layout of the FMM's parity blocks).  The weights come from
+// mms_ctx_set_surrogate (trained by the mms_farnet_* kernels); they are
+// indexed by depth (0 = leaf), the tables here by level of this grid.
+//
+// Three launches on the main stream beside the near field on the side
+// stream: k_fn_up (encoder and the whole upward pass), the resident M2L with
+// per-level tables, and k_fn_down (the whole downward pass, decoder, and the
+// join with the near field).
+constexpr int FN_UP_THREADS = 384;
+constexpr int FN_DOWN_THREADS = 256;
+constexpr int FN_WP = FN_C + 4;  // encoder row pitch in shared memory (floats)
+
+namespace {
+
+// one output k of a block-diagonal map: sum_j T[blk][j][k] x[j] (T one
+// operator of [even NE x NE | odd NO x NO], input-major)
+// (T and x in shared memory)
+__device__ __forceinline__ float fn_apply(const float *T, const float *x, int k)
+{
+    if (k < FN_NE) {
+        float acc = 0.f;
+#pragma unroll
+        for (int j = 0; j < FN_NE; j++) acc = fmaf(T[j * FN_NE + k], x[j], acc);
+        return acc;
+    }
+    const int kk = k - FN_NE;
+    const float *To = T + FN_NE * FN_NE;
+    float acc = 0.f;
+#pragma unroll
+    for (int j = 0; j < FN_NO; j++) acc = fmaf(To[j * FN_NO + kk], x[FN_NE + j], acc);
+    return acc;
+}
+
+// stage n floats (n % 4 == 0, 16-byte aligned) into shared memory with
+// asynchronous copies; commit only (the caller waits)
+__device__ __forceinline__ void fn_stage(float *dst, const float *src, int n)
+{
+    for (int i = threadIdx.x * 4; i < n; i += blockDim.x * 4) umma::cp_async16(umma::smem_u32(dst + i), src + i, true);
+}
+
+// Encoder and upward pass.  CTA = one box of level cb = max(2, L - 2), i.e.
+// gs x gs leaf boxes (gs = 2^(L - cb) <= 4): their charges and the encoder
+// weights are staged in shared memory, the leaf multipoles and every level
+// up to cb formed there and written out.  Levels above cb: the CTA that
+// completes the fourth child of a box forms that box (an arrival counter per
+// box; writers fence their stores before they arrive, the last arriver
+// fences before it reads the siblings through L2), and so on up to level 2.
+// No CTA waits for another.
+__global__ void __launch_bounds__(FN_UP_THREADS) k_fn_up(const float *__restrict__ rho, const float *__restrict__ W,
+                                                         const float *__restrict__ Tm2m, float *__restrict__ Mall,
+                                                         const long long *__restrict__ lev_off,
+                                                         unsigned *__restrict__ ctr, FmmDev f, int cb)
+{
+    pdl_begin();
+    extern __shared__ __align__(16) float fsm[];
+    const int gs = 1 << (f.L - cb), G = gs * gs, ncb = 1 << cb;
+    const int cbx = blockIdx.x % ncb, cby = blockIdx.x / ncb;  // the CTA's box at level cb
+    const int bx0 = cbx * gs, by0 = cby * gs;                  // its first leaf box
+    float *Ws = fsm;                       // [NR][FN_WP]: encoder rows, padded (conflict-free 16-byte reads)
+    float *Ts = Ws + FN_NR * FN_WP;        // M2M tables of parent levels 2 .. L-1: [L-2][4][OSZ]
+    float *q = Ts + (f.L - 2) * 4 * FN_OSZ;  // [G][C]
+    float *mb = q + G * FN_C;              // multipoles of levels L .. cb, G NR + G/4 NR + ...
+    __shared__ int s_last;
+    for (int i = threadIdx.x; i < FN_NR * FN_C / 4; i += blockDim.x) {
+        const int k = i / (FN_C / 4), c4 = i % (FN_C / 4);
+        umma::cp_async16(umma::smem_u32(Ws + k * FN_WP + 4 * c4), W + k * FN_C + 4 * c4, true);
+    }
+    fn_stage(Ts, Tm2m, (f.L - 2) * 4 * FN_OSZ);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // charges, a region row at a time (consecutive threads on consecutive x);
+    // every load of a thread is issued before the first store
+    const int rw = gs * FN_S, ne = FN_Z * rw * rw;
+    constexpr int QR = (FN_Z * 32 * 32 + FN_UP_THREADS - 1) / FN_UP_THREADS;
+    float qv[QR];
+#pragma unroll
+    for (int r = 0; r < QR; r++) {
+        const int e = threadIdx.x + r * blockDim.x;
+        const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
+        const int x = bx0 * FN_S + rx, y = by0 * FN_S + ry;
+        qv[r] = (e < ne && x < f.X && y < f.Y) ? __ldg(&rho[((long long)lz * f.Y + y) * f.X + x]) : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < QR; r++) {
+        const int e = threadIdx.x + r * blockDim.x;
+        if (e >= ne) break;
+        const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
+        const int b = (ry / FN_S) * gs + rx / FN_S, c = lz * FN_S * FN_S + (ry % FN_S) * FN_S + rx % FN_S;
+        q[b * FN_C + c] = qv[r];
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    // encoder: four interleaved chains per output
+    const long long offL = lev_off[f.L];
+    for (int o = threadIdx.x; o < G * FN_NR; o += blockDim.x) {
+        const int b = o / FN_NR, k = o % FN_NR;
+        const float4 *qb = reinterpret_cast<const float4 *>(q + b * FN_C);
+        const float4 *wk = reinterpret_cast<const float4 *>(Ws + k * FN_WP);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 8
+        for (int c4 = 0; c4 < FN_C / 4; c4++) {
+            const float4 wv = wk[c4], qv4 = qb[c4];
+            a0 = fmaf(wv.x, qv4.x, a0);
+            a1 = fmaf(wv.y, qv4.y, a1);
+            a2 = fmaf(wv.z, qv4.z, a2);
+            a3 = fmaf(wv.w, qv4.w, a3);
+        }
+        const float v = (a0 + a1) + (a2 + a3);
+        mb[o] = v;
+        const int bx = bx0 + b % gs, by = by0 + b / gs;
+        Mall[(offL + (long long)by * f.nb + bx) * FN_NR + k] = v;
+    }
+    __syncthreads();
+    // levels L-1 .. cb inside the CTA
+    const float *child = mb;
+    float *par = mb + G * FN_NR;
+    int gc = gs;
+    for (int l = f.L - 1; l >= cb; l--) {
+        const int gp = gc / 2, n = 1 << l;
+        const float *T = Ts + (l - 2) * 4 * FN_OSZ;
+        const int px0 = bx0 >> (f.L - l), py0 = by0 >> (f.L - l);
+        for (int o = threadIdx.x; o < gp * gp * FN_NR; o += blockDim.x) {
+            const int p = o / FN_NR, k = o % FN_NR, px = p % gp, py = p / gp;
+            float v = 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                v += fn_apply(T + c * FN_OSZ, child + ((2 * py + (c >> 1)) * gc + 2 * px + (c & 1)) * FN_NR, k);
+            par[o] = v;
+            Mall[(lev_off[l] + (long long)(py0 + py) * n + px0 + px) * FN_NR + k] = v;
+        }
+        __syncthreads();
+        child = par;
+        par += gp * gp * FN_NR;
+        gc = gp;
+    }
+    // levels above cb: the last of four siblings to finish forms the parent
+    int bxl = cbx, byl = cby;
+    for (int l = cb - 1; l >= 2; l--) {
+        __threadfence();  // this CTA's multipoles are visible before it arrives
+        __syncthreads();
+        const int px = bxl >> 1, py = byl >> 1, n = 1 << l, nc = 2 * n;
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(&ctr[lev_off[l] + (long long)py * n + px], 1u);
+            s_last = t == 3;
+        }
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+        float *sib = mb;  // the four children, read through L2
+        for (int i = threadIdx.x; i < 4 * FN_NR; i += blockDim.x) {
+            const int c = i / FN_NR, k = i % FN_NR;
+            sib[i] = __ldcg(&Mall[(lev_off[l + 1] + (long long)(2 * py + (c >> 1)) * nc + 2 * px + (c & 1)) * FN_NR + k]);
+        }
+        __syncthreads();
+        const float *T = Ts + (l - 2) * 4 * FN_OSZ;
+        for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) {
+            float v = 0.f;
+#pragma unroll
+            for (int c = 0; c < 4; c++) v += fn_apply(T + c * FN_OSZ, sib + c * FN_NR, k);
+            Mall[(lev_off[l] + (long long)py * n + px) * FN_NR + k] = v;
+        }
+        if (threadIdx.x == 0) ctr[lev_off[l] + (long long)py * n + px] = 0u;  // ready for the next launch
+        bxl = px;
+        byl = py;
+    }
+}
+
+// Downward pass, decoder and the join with the near field.  CTA = one box of
+// level L - 1 (its 4 leaf boxes; one leaf box when L = 2): the locals of its
+// ancestors from level 2 down (L2L of the parent's final local plus the
+// box's interaction-list local, one box per level), its leaves' locals, then
+// phi = near field (nnear partials, added in order) + V^T l_leaf at every
+// cell of the 16 x 16 x 3 region.
+__global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__restrict__ Lp,
+                                                             const float *__restrict__ Tl2l,
+                                                             const float *__restrict__ V,
+                                                             const float *__restrict__ near, int nnear,
+                                                             long long near_stride, float *__restrict__ phi,
+                                                             const long long *__restrict__ lev_off, FmmDev f)
+{
+    pdl_begin();
+    __shared__ float cur[FN_NR], nxt[FN_NR], leaf[4][FN_NR];
+    extern __shared__ __align__(16) float dsm[];
+    const int L = f.L;
+    float *Vs = dsm;                  // [NR][C]
+    float *Ts = Vs + FN_NR * FN_C;    // L2L tables of parent levels 2 .. L-1
+    float *Lc = Ts + (L > 2 ? (L - 2) * 4 * FN_OSZ : 0);  // interaction-list locals: ancestors 2..L-1, 4 leaves
+    fn_stage(Vs, V, FN_NR * FN_C);
+    if (L > 2) fn_stage(Ts, Tl2l, (L - 2) * 4 * FN_OSZ);
+    if (L > 2) {
+        // the CTA's chain, every load in flight at once: level l (2..L-1) ancestor, then the 4 leaves
+        const int np = 1 << (L - 1), pbx = blockIdx.x % np, pby = blockIdx.x / np;
+        for (int i = threadIdx.x; i < (L + 2) * (FN_NR / 4); i += blockDim.x) {
+            const int r = i / (FN_NR / 4), k4 = i % (FN_NR / 4);
+            long long box;
+            if (r < L - 2) {
+                const int l = r + 2, sh = L - 1 - l;
+                box = lev_off[l] + (long long)(pby >> sh) * (1 << l) + (pbx >> sh);
+            } else {
+                const int c = r - (L - 2);
+                box = lev_off[L] + (long long)(2 * pby + (c >> 1)) * (1 << L) + 2 * pbx + (c & 1);
+            }
+            umma::cp_async16(umma::smem_u32(Lc + r * FN_NR + 4 * k4), Lp + box * FN_NR + 4 * k4, true);
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    int nlf, lx0, ly0;  // leaves handled and the first one
+    if (L <= 2) {
+        // one leaf box per CTA, its local is its interaction-list local
+        const int n = 1 << L;
+        lx0 = blockIdx.x % n;
+        ly0 = blockIdx.x / n;
+        nlf = 1;
+        for (int k = threadIdx.x; k < FN_NR; k += blockDim.x)
+            leaf[0][k] = Lp[(lev_off[L] + (long long)ly0 * n + lx0) * FN_NR + k];
+    } else {
+        const int np = 1 << (L - 1);
+        const int pbx = blockIdx.x % np, pby = blockIdx.x / np;
+        for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) cur[k] = Lc[k];
+        __syncthreads();
+        for (int l = 3; l <= L - 1; l++) {
+            const int sh = L - 1 - l, bx = pbx >> sh, by = pby >> sh;
+            const int c = (by & 1) * 2 + (bx & 1);
+            const float *T = Ts + ((l - 1 - 2) * 4 + c) * FN_OSZ;
+            for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) nxt[k] = Lc[(l - 2) * FN_NR + k] + fn_apply(T, cur, k);
+            __syncthreads();
+            for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) cur[k] = nxt[k];
+            __syncthreads();
+        }
+        lx0 = 2 * pbx;
+        ly0 = 2 * pby;
+        nlf = 4;
+        for (int i = threadIdx.x; i < 4 * FN_NR; i += blockDim.x) {
+            const int c = i / FN_NR, k = i % FN_NR;
+            const float *T = Ts + ((L - 1 - 2) * 4 + c) * FN_OSZ;
+            leaf[c][k] = Lc[(L - 2 + c) * FN_NR + k] + fn_apply(T, cur, k);
+        }
+    }
+    __syncthreads();
+    // decoder + near field over the region, a row at a time
+    const int gw = nlf == 4 ? 2 : 1, rw = gw * FN_S;
+    for (int e = threadIdx.x; e < FN_Z * rw * rw; e += blockDim.x) {
+        const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
+        const int x = lx0 * FN_S + rx, y = ly0 * FN_S + ry;
+        if (x >= f.X || y >= f.Y) continue;
+        const long long cell = ((long long)lz * f.Y + y) * f.X + x;
+        const int b = (ry / FN_S) * gw + rx / FN_S, c = lz * FN_S * FN_S + (ry % FN_S) * FN_S + rx % FN_S;
+        float acc = __ldg(&near[cell]);
+        for (int qn = 1; qn < nnear; qn++) acc += __ldg(&near[qn * near_stride + cell]);
+        const float *lb = leaf[b];
+#pragma unroll 8
+        for (int k = 0; k < FN_NR; k++) acc = fmaf(Vs[k * FN_C + c], lb[k], acc);
+        phi[cell] = acc;
+    }
+}
+
+size_t fn_up_smem(int L)
+{
+    const int cb = std::max(2, L - 2), gs = 1 << (L - cb), G = gs * gs;
+    int nm = 0;
+    for (int g = G; g >= 1; g /= 4) nm += g;
+    return ((size_t)FN_NR * FN_WP + (size_t)std::max(L - 2, 0) * 4 * FN_OSZ + (size_t)G * FN_C +
+            (size_t)std::max(nm, 4) * FN_NR) * sizeof(float);
+}
+
+size_t fn_down_smem(int L)
+{
+    return ((size_t)FN_NR * FN_C + (size_t)std::max(L - 2, 0) * 4 * FN_OSZ + (size_t)(L + 2) * FN_NR) *
+           sizeof(float);
+}
+
+}  // namespace
+
+// Binds a weight vector (indexed by depth) to the context's plan: tables per
+// level of this grid, encoder scaled to physical units (phi = dx^2 net(rho)
+// for cubic cells), work buffers.  Leaf side 8 and 3 layers only.
+int farnet_bind(mms_ctx *ctx, const float *w, long long count)
+{
+    FmmPlan *pl = ctx->fmm;
+    if (!pl) {
+        mms_set_error("surrogate: no FMM plan");
+        return MMS_ERR_ARG;
+    }
+    const FmmDev &f = pl->d;
+    if (f.s != FN_S || f.Z != FN_Z) {
+        mms_set_error("surrogate: the network works on 8 x 8 x 3 leaf boxes (leaf side %d, %d layers given)", f.s,
+                      f.Z);
+        return MMS_ERR_ARG;
+    }
+    if (f.L > FN_DEPTHS + 1) {
+        mms_set_error("surrogate: a grid of %d quadtree levels exceeds the network's %d depths", f.L, FN_DEPTHS);
+        return MMS_ERR_ARG;
+    }
+    const long long need = fn_num_params();
+    if (count != need) {
+        mms_set_error("surrogate: %lld weights given, the network has %lld", count, need);
+        return MMS_ERR_ARG;
+    }
+    if (!m2l_res_supported(FN_NR, FN_NE)) {
+        mms_set_error("surrogate: no resident M2L kernel for width %d", FN_NR);
+        return MMS_ERR_ARG;
+    }
+    const int L = std::max(f.L, 2);
+    const int nlev = L - 1;  // levels 2..L
+    const double sc = ctx->g.dx * ctx->g.dx;
+    std::vector<float> W((size_t)FN_C * FN_NR), V((size_t)FN_NR * FN_C);
+    for (int c = 0; c < FN_C; c++)  // [c][k] -> [k][c]
+        for (int k = 0; k < FN_NR; k++) W[(size_t)k * FN_C + c] = (float)(w[fn_off_W() + c * FN_NR + k] * sc);
+    for (size_t i = 0; i < V.size(); i++) V[i] = w[fn_off_V() + i];
+    std::vector<float> M2L((size_t)nlev * 49 * FN_OSZ), M2M((size_t)std::max(1, nlev - 1) * 4 * FN_OSZ, 0.f),
+        L2L(M2M.size(), 0.f);
+    for (int l = 2; l <= L; l++) {
+        const int d = L - l;
+        memcpy(&M2L[(size_t)(l - 2) * 49 * FN_OSZ], w + fn_off_M2L(d), 49 * FN_OSZ * sizeof(float));
+        if (l < L) {  // parent level l, depth d >= 1
+            memcpy(&M2M[(size_t)(l - 2) * 4 * FN_OSZ], w + fn_off_M2M(d), 4 * FN_OSZ * sizeof(float));
+            memcpy(&L2L[(size_t)(l - 2) * 4 * FN_OSZ], w + fn_off_L2L(d), 4 * FN_OSZ * sizeof(float));
+        }
+    }
+    auto up = [&](float **dst, const std::vector<float> &h) -> int {
+        if (!*dst) {
+            if (cudaMalloc((void **)dst, h.size() * sizeof(float)) != cudaSuccess) {
+                mms_set_error("surrogate: device allocation failed");
+                return MMS_ERR_NOMEM;
+            }
+            pl->bytes += h.size() * sizeof(float);
+        }
+        MMS_CUDA_TRY(cudaMemcpyAsync(*dst, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        return MMS_OK;
+    };
+    MMS_TRY(up(&pl->fnW, W));
+    MMS_TRY(up(&pl->fnV, V));
+    MMS_TRY(up(&pl->fnM2L, M2L));
+    MMS_TRY(up(&pl->fnM2M, M2M));
+    MMS_TRY(up(&pl->fnL2L, L2L));
+    if (!pl->fnM) {
+        const size_t nb = (size_t)std::max(pl->nbox_total, 1LL);
+        if (cudaMalloc((void **)&pl->fnM, nb * FN_NR * sizeof(float)) != cudaSuccess ||
+            cudaMalloc((void **)&pl->fnLp, nb * FN_NR * sizeof(float)) != cudaSuccess ||
+            cudaMalloc((void **)&pl->fnCtr, nb * sizeof(unsigned)) != cudaSuccess) {
+            mms_set_error("surrogate: device allocation failed");
+            return MMS_ERR_NOMEM;
+        }
+        pl->bytes += nb * (2 * FN_NR * sizeof(float) + sizeof(unsigned));
+        MMS_CUDA_TRY(cudaMemsetAsync(pl->fnM, 0, nb * FN_NR * sizeof(float), ctx->stream));
+        MMS_CUDA_TRY(cudaMemsetAsync(pl->fnLp, 0, nb * FN_NR * sizeof(float), ctx->stream));
+        MMS_CUDA_TRY(cudaMemsetAsync(pl->fnCtr, 0, nb * sizeof(unsigned), ctx->stream));
+        MMS_TRY(m2l_res_prepare(FN_NR, FN_NE));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_up, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)fn_up_smem(FN_DEPTHS + 1)));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_up, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_down, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)fn_down_smem(FN_DEPTHS + 1)));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_down, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+    }
+    MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    pl->fn_ready = 1;
+    return MMS_OK;
+}
+
+// surrogate potential: the exact near field on the side stream; the network's
+// three launches on the main one; the last adds the two
 int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
 {
     FmmPlan *pl = ctx->fmm;
-    if (!pl || !ctx->sno) {
+    if (!pl || !pl->fn_ready) {
         mms_set_error("surrogate solver: no weights bound (mms_ctx_set_surrogate)");
         return MMS_ERR_NOT_READY;
     }
     const FmmDev &f = pl->d;
-    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
     MMS_CUDA_TRY(cudaEventRecord(pl->ev_fork, ctx->stream));
     MMS_CUDA_TRY(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
-    MMS_TRY(p2p_launch(f, nbx, nby, rho, pl->Gn, pl->near, pl->side));
+    MMS_TRY(near_launch(ctx, rho, pl->side));
     MMS_LAUNCH_CHECK(ctx);
     MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
-    // u = rho dx / Ms in, phi_far = (Ms dx) y out (cubic cells)
-    const double Ms = ctx->p.Ms > 0 ? ctx->p.Ms : 1.0;
-    return sno_launch_far(ctx->sno, ctx->stream, rho, (float)(ctx->g.dx / Ms), phi, pl->near,
-                          (float)(Ms * ctx->g.dx), pl->ev_join, &ctx->launches);
+    const float *near = pl->p2p_tc ? pl->near3 : pl->near;
+    const int nnear = pl->p2p_tc ? 3 : 1;
+    if (f.L < 2) {
+        // no far field: every box is in every other's near zone
+        MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
+        k_sum_parts<<<(unsigned)div_up(ctx->N, 256), 256, 0, ctx->stream>>>(near, nnear, ctx->N, phi);
+        MMS_LAUNCH_CHECK(ctx);
+        return MMS_OK;
+    }
+    const int cb = std::max(2, f.L - 2);
+    MMS_CUDA_TRY(launch_k(k_fn_up, dim3(1u << (2 * cb)), dim3(FN_UP_THREADS), fn_up_smem(f.L), ctx->stream, rho,
+                          (const float *)pl->fnW, (const float *)pl->fnM2M, pl->fnM, (const long long *)pl->lev_dev,
+                          pl->fnCtr, f, cb));
+    MMS_LAUNCH_CHECK(ctx);
+    FmmDev fn = f;
+    fn.NR = FN_NR;
+    fn.NE = FN_NE;
+    MMS_TRY(m2l_res_launch(fn, pl->n_res_items, pl->fnM, pl->fnLp, pl->fnM2L, pl->res_items, pl->lev_dev, ctx->stream,
+                           49LL * FN_OSZ));
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
+    const unsigned ndown = f.L > 2 ? 1u << (2 * (f.L - 1)) : 1u << (2 * f.L);
+    MMS_CUDA_TRY(launch_k(k_fn_down, dim3(ndown), dim3(FN_DOWN_THREADS), fn_down_smem(f.L), ctx->stream,
+                          (const float *)pl->fnLp,
+                          (const float *)pl->fnL2L, (const float *)pl->fnV, near, nnear, (long long)ctx->N, phi,
+                          (const long long *)pl->lev_dev, f));
+    MMS_LAUNCH_CHECK(ctx);
+    return MMS_OK;
 }
 
 int fmm_split_target(const mms_ctx *ctx, void **hi, void **lo, int *nbx, int *nby)

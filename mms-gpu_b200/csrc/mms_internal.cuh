@@ -101,8 +101,8 @@ struct mms_ctx {
 
     FmmPlan *fmm = nullptr;
 
-    // surrogate solver (MMS_SOLVER_SURROGATE)
-    mms_sno *sno = nullptr;
+    // surrogate solver (MMS_SOLVER_SURROGATE): weights bound to the FMM plan
+    bool sur_bound = false;
     int sur_every = 0;
     double sur_tol = 1e-3;
     bool sur_active = false;                    // false: the FMM took over
@@ -143,12 +143,9 @@ int launch_potential_direct(mms_ctx *ctx, const float *rho, float *phi);
 int fmm_plan_create(mms_ctx *ctx);
 int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi);
 int launch_potential_split(mms_ctx *ctx, const float *rho, float *phi, float *near);
-// network forward (sno.cu): phi = near + out_scale * net(in_scale * rho); the
-// head waits for `wait_before_head` (may be NULL)
-int sno_launch_far(mms_sno *n, cudaStream_t st, const float *rho, float in_scale, float *phi, const float *near,
-                   float out_scale, cudaEvent_t wait_before_head, int64_t *launches);
-int sno_error_flag(mms_sno *n, cudaStream_t st);
-void sno_set_fast(mms_sno *n, bool fast);
+// binds the learned far-field network's weights (a vector indexed by depth,
+// farnet.cuh) to the context's FMM plan (leaf 8, 3 layers)
+int farnet_bind(mms_ctx *ctx, const float *w, long long count);
 // rel-L2 |a - b| / |b| over n floats (tune.cu); synchronises ctx->stream
 int rel_l2_dev(mms_ctx *ctx, const float *a, const float *b, long long n, double *out);
 void fmm_plan_destroy(mms_ctx *ctx);

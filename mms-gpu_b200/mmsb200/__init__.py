@@ -121,16 +121,16 @@ SIGNATURES = {
     "mms_ens_run_fixed": (_I, [_VP, _D, _I, _I]),
     "mms_ens_sync": (_I, [_VP]),
     "mms_fmm_stage_times": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_D)]),
-    "mms_sno_num_params": (ctypes.c_longlong, []),
-    "mms_sno_create": (_I, [_I, _I, _I, _I, ctypes.POINTER(_VP)]),
-    "mms_sno_destroy": (None, [_VP]),
-    "mms_sno_set_weights": (_I, [_VP, _VP, ctypes.c_longlong]),
-    "mms_sno_get_weights": (_I, [_VP, _VP, ctypes.c_longlong, _I]),
-    "mms_sno_forward_dev": (_I, [_VP, _VP, _VP, _I]),
-    "mms_sno_gradient": (_I, [_VP, _VP, _VP, _I, _VP, ctypes.POINTER(_D)]),
-    "mms_sno_train_step": (_I, [_VP, _VP, _VP, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
-                                ctypes.POINTER(_D)]),
-    "mms_sno_device_bytes": (ctypes.c_longlong, [_VP]),
+    "mms_farnet_num_params": (ctypes.c_longlong, []),
+    "mms_farnet_create": (_I, [_I, _I, _I, ctypes.POINTER(_VP)]),
+    "mms_farnet_destroy": (None, [_VP]),
+    "mms_farnet_set_weights": (_I, [_VP, _VP, ctypes.c_longlong]),
+    "mms_farnet_get_weights": (_I, [_VP, _VP, ctypes.c_longlong]),
+    "mms_farnet_forward_dev": (_I, [_VP, _VP, _VP, _I]),
+    "mms_farnet_gradient": (_I, [_VP, _VP, _VP, _VP, _I, _VP, ctypes.POINTER(_D)]),
+    "mms_farnet_train_step": (_I, [_VP, _VP, _VP, _VP, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                   ctypes.c_float, ctypes.POINTER(_D)]),
+    "mms_farnet_device_bytes": (ctypes.c_longlong, [_VP]),
     "mms_ctx_set_surrogate": (_I, [_VP, _VP, ctypes.c_longlong, _I, _D, _I]),
     "mms_surrogate_check": (_I, [_VP, ctypes.POINTER(_D)]),
     "mms_surrogate_stats": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong),
@@ -333,7 +333,7 @@ class Context:
         """FMM potential and its exact near-field part (device arrays)"""
         _check(load().mms_potential_split_dev(self.h, _ptr(rho), _ptr(phi), _ptr(near)))
 
-    def set_surrogate(self, weights, check_every=50, tol=1e-3, fast=True):
+    def set_surrogate(self, weights, check_every=50, tol=1e-3, fast=False):
         w = np.ascontiguousarray(weights, np.float32)
         _check(load().mms_ctx_set_surrogate(self.h, _ptr(w), w.size, check_every, tol, int(fast)))
 
@@ -420,25 +420,26 @@ class Context:
         return rows, st
 
 
-class SNO:
-    """The surrogate far-field network (mms_sno) for [batch][Z][Y][X] cell
+class FarNet:
+    """The learned far-field network (mms_farnet) for [batch][3][Y][X] cell
     arrays on the current CUDA device: dimensionless charge u = rho dx / Ms in,
-    dimensionless far-field potential phi_far / (Ms dx) out."""
+    dimensionless far-field potential phi_far / (Ms dx) out (the near field
+    over each 8 x 8 x 3 leaf box's 3 x 3 neighbourhood excluded)."""
 
-    def __init__(self, xdim, ydim, zdim, batch=1):
-        self.shape = (zdim, ydim, xdim)
+    def __init__(self, xdim, ydim, batch=1):
+        self.shape = (3, ydim, xdim)
         self.batch = batch
         h = _VP()
-        _check(load().mms_sno_create(xdim, ydim, zdim, batch, ctypes.byref(h)))
+        _check(load().mms_farnet_create(xdim, ydim, batch, ctypes.byref(h)))
         self.h = h
 
     @staticmethod
     def num_params():
-        return int(load().mms_sno_num_params())
+        return int(load().mms_farnet_num_params())
 
     def close(self):
         if self.h:
-            load().mms_sno_destroy(self.h)
+            load().mms_farnet_destroy(self.h)
             self.h = None
 
     def __enter__(self):
@@ -455,28 +456,29 @@ class SNO:
 
     def set_weights(self, w):
         w = np.ascontiguousarray(w, np.float32)
-        _check(load().mms_sno_set_weights(self.h, _ptr(w), w.size))
+        _check(load().mms_farnet_set_weights(self.h, _ptr(w), w.size))
 
-    def get_weights(self, bf16_rounded=False):
+    def get_weights(self):
         w = np.empty(self.num_params(), np.float32)
-        _check(load().mms_sno_get_weights(self.h, _ptr(w), w.size, int(bf16_rounded)))
+        _check(load().mms_farnet_get_weights(self.h, _ptr(w), w.size))
         return w
 
     def forward_dev(self, u, out, nbatch=1):
-        _check(load().mms_sno_forward_dev(self.h, _ptr(u), _ptr(out), nbatch))
+        _check(load().mms_farnet_forward_dev(self.h, _ptr(u), _ptr(out), nbatch))
 
-    def gradient(self, u, far, nbatch=1):
+    def gradient(self, u, far, nrm2, nbatch=1):
         g = np.empty(self.num_params(), np.float32)
         loss = ctypes.c_double()
-        _check(load().mms_sno_gradient(self.h, _ptr(u), _ptr(far), nbatch, _ptr(g), ctypes.byref(loss)))
+        _check(load().mms_farnet_gradient(self.h, _ptr(u), _ptr(far), _ptr(nrm2), nbatch, _ptr(g),
+                                          ctypes.byref(loss)))
         return loss.value, g
 
-    def train_step(self, u, far, nbatch, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+    def train_step(self, u, far, nrm2, nbatch, lr, beta1=0.9, beta2=0.999, eps=1e-12):
         loss = ctypes.c_double()
-        _check(load().mms_sno_train_step(self.h, _ptr(u), _ptr(far), nbatch, lr, beta1, beta2, eps,
-                                         ctypes.byref(loss)))
+        _check(load().mms_farnet_train_step(self.h, _ptr(u), _ptr(far), _ptr(nrm2), nbatch, lr, beta1, beta2, eps,
+                                            ctypes.byref(loss)))
         return loss.value
 
     def device_bytes(self):
-        return int(load().mms_sno_device_bytes(self.h))
+        return int(load().mms_farnet_device_bytes(self.h))
 

@@ -1,13 +1,17 @@
-"""Training and use of the surrogate far-field network (mms_sno).
+"""Training and use of the learned far-field network (mms_farnet).
 
-Training pairs are (u, far) = (rho dx / Ms, (phi_FMM - phi_near) / (Ms dx))
-taken along LLG trajectories that the library itself integrates: instances of
-64..256 cells a side (disc lattices, discs, ellipses, rectangles, block-masked
-films; in-plane, per-dot, vortex or random initial states; constant or ramped
-in-plane fields up to 50 mT) placed in a fixed canvas, stepped with the FMM,
-and evaluated every few steps by a high-order FMM (P = 8, leaf 4) whose exact
-near field (mms_potential_split_dev) is subtracted.  The network is then fitted
-by the library's own forward / backward / Adam kernels (mms_sno_train_step).
+Training pairs are (u, far, nrm2): u = rho dx / Ms, far = (phi_FMM -
+phi_near) / (Ms dx) and nrm2 = |phi_FMM / (Ms dx)|^2, taken along LLG
+trajectories that the library itself integrates: instances of 64..256 cells a
+side (disc lattices, discs, ellipses, rectangles, block-masked films;
+in-plane, per-dot, vortex or random initial states; constant or ramped
+in-plane fields up to 50 mT) placed in a 256 x 256 x 3 canvas, stepped with
+the FMM, and evaluated every few steps by a high-order FMM (P = 8, leaf 8,
+within ~4e-6 of the exact sum) whose exact near field
+(mms_potential_split_dev) is subtracted.  The network starts from nested SVD
+bases of the 1/r interactions (farnet.h2_init) and is fitted by the library's
+own forward / adjoint / tensor-core weight-gradient / Adam kernels
+(mms_farnet_train_step) on the relative error of the total potential.
 
 Everything here runs through the C ABI; torch only holds device buffers.
 """
@@ -19,12 +23,13 @@ import time
 
 import numpy as np
 
-from . import (SNO, SOLVER_FMM, Context, Grid, geometry, make_params, make_solver)
+from . import (SOLVER_FMM, Context, FarNet, Grid, farnet, geometry, make_params, make_solver)
 
 MS = geometry.MS_PERMALLOY
 DX = 5e-9
+LEAF = 8
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights")
-DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "sno_patch4_c32_l4.npz")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "farnet_w24_d5.npz")
 
 
 # ---- training geometries ------------------------------------------------------
@@ -83,15 +88,17 @@ def _field(rng):
 
 def generate_pairs(n_pairs, X=256, Y=256, Z=3, snaps_per_run=50, steps_between=10, dt=1e-13, seed=2010,
                    target_order=8, progress=None):
-    """n_pairs training pairs as two torch tensors [n, Z, Y, X] (float32, cuda)"""
+    """n_pairs training pairs: torch tensors U, F [n, Z, Y, X] and N2 [n]
+    (float32, cuda)"""
     import torch
     rng = np.random.Generator(np.random.Philox(seed))
     N = X * Y * Z
     U = torch.empty((n_pairs, Z, Y, X), dtype=torch.float32, device="cuda")
     F = torch.empty_like(U)
+    N2 = torch.empty(n_pairs, dtype=torch.float32, device="cuda")
     grid = Grid(X, Y, Z, DX, DX, DX)
-    dyn = Context(grid, make_params(), make_solver(SOLVER_FMM, 4, 4))
-    tgt = Context(grid, make_params(), make_solver(SOLVER_FMM, target_order, 4))
+    dyn = Context(grid, make_params(), make_solver(SOLVER_FMM, 4, LEAF))
+    tgt = Context(grid, make_params(), make_solver(SOLVER_FMM, target_order, LEAF))
     Mdev = torch.empty((N, 3), dtype=torch.float64, device="cuda")
     rho = torch.empty(N, dtype=torch.float32, device="cuda")
     phi = torch.empty_like(rho)
@@ -114,6 +121,7 @@ def generate_pairs(n_pairs, X=256, Y=256, Z=3, snaps_per_run=50, steps_between=1
                 tgt.potential_split_dev(rho, phi, near)
                 U[k] = (rho * (DX / MS)).view(Z, Y, X)
                 F[k] = ((phi - near) / (MS * DX)).view(Z, Y, X)
+                N2[k] = ((phi / (MS * DX)).double() ** 2).sum().float()
                 k += 1
             if progress:
                 progress(k, time.time() - t0)
@@ -121,13 +129,14 @@ def generate_pairs(n_pairs, X=256, Y=256, Z=3, snaps_per_run=50, steps_between=1
     finally:
         dyn.close()
         tgt.close()
-    return U, F
+    return U, F, N2
 
 
 def benchmark_pairs(n_pairs, seed=777, X=256, Y=256, Z=3, steps_between=20, dt=1e-13):
     """held-out pairs of the benchmark workload itself (8 x 8 disc lattice,
     r = 12, pitch 32, per-dot random in-plane M, B_x ramp -50..+50 mT / 10 ns),
-    seeds disjoint from training"""
+    seeds disjoint from training: U, F, N2 as generate_pairs, plus the total
+    potential P [n, Z, Y, X] (dimensionless)"""
     import torch
     grid = Grid(X, Y, Z, DX, DX, DX)
     N = X * Y * Z
@@ -139,8 +148,8 @@ def benchmark_pairs(n_pairs, seed=777, X=256, Y=256, Z=3, steps_between=20, dt=1
     phi = torch.empty_like(rho)
     near = torch.empty_like(rho)
     prm = make_params(external=True, hext_t=[0.0, 1e-8], hext_b=[[-0.05, 0, 0], [0.05, 0, 0]])
-    with Context(grid, prm, make_solver(SOLVER_FMM, 4, 4)) as dyn, \
-            Context(grid, make_params(), make_solver(SOLVER_FMM, 8, 4)) as tgt:
+    with Context(grid, prm, make_solver(SOLVER_FMM, 4, LEAF)) as dyn, \
+            Context(grid, make_params(), make_solver(SOLVER_FMM, 8, LEAF)) as tgt:
         per_run = 10
         for k in range(n_pairs):
             if k % per_run == 0:
@@ -154,66 +163,36 @@ def benchmark_pairs(n_pairs, seed=777, X=256, Y=256, Z=3, steps_between=20, dt=1
             U[k] = (rho * (DX / MS)).view(Z, Y, X)
             F[k] = ((phi - near) / (MS * DX)).view(Z, Y, X)
             P[k] = (phi / (MS * DX)).view(Z, Y, X)
-    return U, F, P
+    N2 = (P.double() ** 2).flatten(1).sum(1).float()
+    return U, F, N2, P
 
 
 # ---- training -------------------------------------------------------------------
 
-def layer_shapes():
-    """(kind, taps, cin, cout) of every layer in weight order: conv3 x -> a0;
-    per level 1..3 down + conv3; bottleneck conv3; per level 2..0 up + conv3;
-    point head (the library's network, mms_sno)"""
-    L = [("conv3", 27, 16, 32)]
-    for _ in range(3):
-        L += [("down", 4, 32, 32), ("conv3", 27, 32, 32)]
-    L.append(("conv3", 27, 32, 32))
-    for _ in range(3):
-        L += [("up", 4, 32, 32), ("conv3", 27, 32, 32)]
-    L.append(("point", 1, 32, 16))
-    return L
-
-
-def init_weights(seed=1):
-    """per-layer uniform +-sqrt(3 / fan_in), seeded Philox; fan_in = taps x cin
-    (cin for an up transfer, where each output takes one tap)"""
-    g = np.random.Generator(np.random.Philox(seed))
-    parts = []
-    for kind, taps, cin, cout in layer_shapes():
-        fan_in = cin if kind == "up" else taps * cin
-        lim = np.sqrt(3.0 / fan_in)
-        parts.append(g.uniform(-lim, lim, cout * taps * cin))
-    w = np.concatenate(parts).astype(np.float32)
-    assert w.size == SNO.num_params()
-    return w
-
-
-def evaluate(net, U, F, P=None, batch=8):
-    """mean and max rel-L2 of the network's far field (and of the total
-    potential when P, the full potential, is given) over the pairs"""
+def evaluate(net, U, F, N2, P=None, batch=8):
+    """mean and max rel-L2 of the total potential (far-field error over
+    |phi|) over the pairs"""
     import torch
     out = torch.empty((batch,) + tuple(U.shape[1:]), dtype=torch.float32, device="cuda")
-    ef, et = [], []
+    et = []
     for i in range(0, U.shape[0], batch):
         nb = min(batch, U.shape[0] - i)
         net.forward_dev(U[i:i + nb], out, nb)
         d = (out[:nb] - F[i:i + nb]).double()
-        ef += (d.flatten(1).norm(dim=1) / F[i:i + nb].double().flatten(1).norm(dim=1)).tolist()
-        if P is not None:
-            et += (d.flatten(1).norm(dim=1) / P[i:i + nb].double().flatten(1).norm(dim=1)).tolist()
-    r = dict(far_mean=float(np.mean(ef)), far_max=float(np.max(ef)))
-    if P is not None:
-        r.update(total_mean=float(np.mean(et)), total_max=float(np.max(et)))
-    return r
+        et += (d.flatten(1).norm(dim=1) / N2[i:i + nb].double().sqrt()).tolist()
+    return dict(total_mean=float(np.mean(et)), total_max=float(np.max(et)))
 
 
-def train(U, F, steps, batch=8, lr_max=2e-3, lr_min=1e-5, warmup=0.03, seed=1, weights=None, val=None,
-          log_every=500, log=print):
-    """fits a fresh (or the given) network to the pairs with Adam on a
-    warm-up + cosine schedule; returns (weights, history)"""
+def train(U, F, N2, steps, batch=8, lr_max=3e-5, lr_min=3e-7, warmup=0.02, seed=1, weights=None, val=None,
+          log_every=250, log=print):
+    """fits the network (from `weights`, else the nested-SVD start) to the
+    pairs with Adam on a warm-up + cosine schedule; returns (weights, history,
+    start weights); with `val`, the weights of the best validation mean"""
     import torch
     Z, Y, X = U.shape[1:]
-    net = SNO(X, Y, Z, batch)
-    net.set_weights(init_weights(seed) if weights is None else weights)
+    net = FarNet(X, Y, batch)
+    w0 = np.asarray(farnet.h2_init() if weights is None else weights, np.float32)
+    net.set_weights(w0)
     g = torch.Generator(device="cpu").manual_seed(seed)
     hist = []
     t0 = time.time()
@@ -222,6 +201,15 @@ def train(U, F, steps, batch=8, lr_max=2e-3, lr_min=1e-5, warmup=0.03, seed=1, w
     pos = 0
     ub = torch.empty((batch, Z, Y, X), dtype=torch.float32, device="cuda")
     fb = torch.empty_like(ub)
+    nb2 = torch.empty(batch, dtype=torch.float32, device="cuda")
+    best = (None, None)
+    if val is not None:
+        rec = dict(step=-1, s=0.0)
+        rec.update(evaluate(net, *val))
+        hist.append(rec)
+        best = (rec["total_mean"], net.get_weights())
+        if log:
+            log(rec)
     for it in range(steps):
         if pos + batch > n:
             perm = torch.randperm(n, generator=g)
@@ -230,22 +218,25 @@ def train(U, F, steps, batch=8, lr_max=2e-3, lr_min=1e-5, warmup=0.03, seed=1, w
         pos += batch
         torch.index_select(U, 0, idx, out=ub)
         torch.index_select(F, 0, idx, out=fb)
+        torch.index_select(N2, 0, idx, out=nb2)
         w = it / max(1, steps - 1)
         if w < warmup:
             lr = lr_max * (it + 1) / (warmup * steps)
         else:
             lr = lr_min + 0.5 * (lr_max - lr_min) * (1 + math.cos(math.pi * (w - warmup) / (1 - warmup)))
-        loss = net.train_step(ub, fb, batch, lr)
+        loss = net.train_step(ub, fb, nb2, batch, lr)
         if it % log_every == 0 or it == steps - 1:
-            rec = dict(step=it, loss=loss, lr=lr, s=time.time() - t0)
+            rec = dict(step=it, loss_rel=math.sqrt(max(loss, 0.0)), lr=lr, s=time.time() - t0)
             if val is not None:
                 rec.update(evaluate(net, *val))
+                if rec["total_mean"] < best[0]:
+                    best = (rec["total_mean"], net.get_weights())
             hist.append(rec)
             if log:
                 log(rec)
-    w = net.get_weights()
+    w = best[1] if best[1] is not None else net.get_weights()
     net.close()
-    return w, hist
+    return w, hist, w0
 
 
 def save_weights(path, w, meta):
@@ -267,12 +258,12 @@ def main(argv=None):
     import json
 
     import torch
-    ap = argparse.ArgumentParser(description="train the surrogate far-field network")
-    ap.add_argument("--pairs", type=int, default=20000)
-    ap.add_argument("--steps", type=int, default=20000)
+    ap = argparse.ArgumentParser(description="train the learned far-field network")
+    ap.add_argument("--pairs", type=int, default=4000)
+    ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=8)
-    ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--val", type=int, default=100)
+    ap.add_argument("--lr", type=float, default=3e-5)
+    ap.add_argument("--val", type=int, default=40)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--log", default=None)
     a = ap.parse_args(argv)
@@ -286,16 +277,18 @@ def main(argv=None):
             logf.flush()
 
     t0 = time.time()
-    U, F = generate_pairs(a.pairs, progress=lambda k, s: k % 2000 < 50 and log(dict(pairs=k, s=round(s, 1))))
+    U, F, N2 = generate_pairs(a.pairs, progress=lambda k, s: k % 1000 < 50 and log(dict(pairs=k, s=round(s, 1))))
     log(dict(generated=a.pairs, s=time.time() - t0))
-    val = benchmark_pairs(a.val)
-    w, hist = train(U, F, a.steps, a.batch, a.lr, val=val, log=log)
+    Uv, Fv, N2v, _ = benchmark_pairs(a.val)
+    w, hist, w0 = train(U, F, N2, a.steps, a.batch, a.lr, val=(Uv, Fv, N2v), log=log)
     del U, F
     torch.cuda.empty_cache()
-    final = hist[-1]
-    save_weights(a.out, w, dict(pairs=a.pairs, steps=a.steps, batch=a.batch, lr=a.lr, patch=4, channels=32,
-                                levels=4, val_far_mean=final.get("far_mean", -1),
-                                val_total_mean=final.get("total_mean", -1)))
+    start = hist[0]
+    best = min((h for h in hist if "total_mean" in h), key=lambda h: h["total_mean"])
+    save_weights(a.out, w, dict(pairs=a.pairs, steps=a.steps, batch=a.batch, lr=a.lr, width=farnet.NR,
+                                even=farnet.NE, odd=farnet.NO, depths=farnet.DEPTHS,
+                                val_start_mean=start["total_mean"], val_start_max=start["total_max"],
+                                val_mean=best["total_mean"], val_max=best["total_max"], val_best_step=best["step"]))
     log(dict(saved=a.out, total_s=time.time() - t0))
 
 
