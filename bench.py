@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the learned far-field measurement")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble measurement")
     ap.add_argument("--workload", choices=["single", "ensemble"], default="single",
                     help="single: the 256x256x3 metric; ensemble: the batched-ensemble configuration")
     ap.add_argument("--ensemble-size", type=int, default=512)
@@ -353,6 +354,14 @@ def run_ours(args):
         dev_mat = torch.empty(host_mat.shape, dtype=torch.uint8, device="cuda")
         out_M = torch.empty_like(host_M).pin_memory()
         t = 0.0
+        # one untimed round trip first: a state set from the host has no
+        # potential yet, so these steps run the evaluate-first step graph,
+        # captured here (4 field evaluations per step either way)
+        dev_M.copy_(host_M, non_blocking=True)
+        dev_mat.copy_(host_mat, non_blocking=True)
+        ctx.state_set_dev(dev_mat, dev_M, t)
+        ctx.run_fixed(args.dt, 1, use_graph=True)
+        ctx.sync()
         ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(args.steps)]
         for k in range(args.steps):
@@ -371,11 +380,19 @@ def run_ours(args):
         e2e = {"value": ws * args.steps / (e2e_ms * 1e-3), "unit": "steps/s",
                "h2d_bytes_per_step": int(host_M.numel() * 8 + host_mat.numel()),
                "d2h_bytes_per_step": int(out_M.numel() * 8),
-               "path": "mms_state_set_dev + mms_run_fixed(1 step) + mms_state_get_dev, pinned host copies"}
+               "path": "mms_state_set_dev + mms_run_fixed(1 step) + mms_state_get_dev, pinned host copies; "
+                       "4 field evaluations per step, as in the device-timed steps"}
 
     sur = None
     if args.solver == "fmm" and not args.no_surrogate:
         sur = surrogate_block(args, grid, params, mask, M, stream, flush, value)
+
+    # the batched-ensemble configuration, measured in the same run (every rank
+    # runs its cost partition of the instances; rank 0 reports)
+    ens = None
+    if not args.no_ensemble:
+        em = ensemble_measure(args, stream, flush, ws, rank)
+        ens = ensemble_summary(args, em, max_over_ranks(ws, em["ms_total"]), ws, fma_peak)
 
     base = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -410,6 +427,8 @@ def run_ours(args):
             "e2e": e2e, "cpu_baseline": base}
     if sur is not None:
         line["surrogate"] = sur
+    if ens is not None:
+        line["ensemble"] = ens
     if acc is not None:
         line["accuracy"] = {"demag_phi_rel_l2_vs_direct": acc,
                             "note": "direct = exact FP32 table + compensated sum, itself <= 2e-6 from FP64"}
@@ -564,80 +583,98 @@ def fmm_roofline(ctx, pot_ms, fma_peak, rho, phi):
     return roof
 
 
-def run_ensemble(args):
-    """Batched ensemble: `--ensemble-size` independent simulations (sides 16..64
-    in steps of 8, x3 layers, rectangle/disc/ellipse masks, random M, random
-    in-plane |B| <= 50 mT; dt = 1e-13 s), one CUDA graph per ensemble step.
-    Under torchrun the instances are partitioned over ranks by cost with no
-    collective on the data path; value = ensemble steps/s of the whole job."""
+def ensemble_measure(args, stream, flush, ws=1, rank=0):
+    """The batched-ensemble configuration: `--ensemble-size` independent
+    simulations (sides 16..64 in steps of 8, x3 layers, rectangle/disc/ellipse
+    masks, random M, random in-plane |B| <= 50 mT; dt = 1e-13 s), one CUDA
+    graph per ensemble step, the direct kernel's shape autotuned first.  Under
+    torchrun the instances are partitioned over ranks by cost with no
+    collective on the data path.  Returns the measurement (this rank's device
+    time; the caller takes the max over ranks)."""
     import torch
     import mmsb200
     from mmsb200 import geometry
     from mmsb200.ensemble import Ensemble, cost, partition
-    ws, rank, local = dist_init()
     dims, masks, Ms, bext = geometry.ensemble_instances(args.ensemble_size, seed=2010)
     mine = partition([cost(d) for d in dims], ws, rank)
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
     ens = Ensemble([dims[i] for i in mine], (5e-9, 5e-9, 5e-9), mmsb200.make_params(external=True),
                    bext=[bext[i] for i in mine], stream=stream.cuda_stream)
     ens.state_set([masks[i] for i in mine], [Ms[i] for i in mine])
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ew, q, direct_ms = ens.autotune(5)
+    steps = max(args.steps, 20)
     ens.run_fixed(args.dt, max(args.warmup, 3), use_graph=True)
     ens.sync()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    clocks = ClockSampler(local)
-    barrier(ws)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     torch.cuda.synchronize()
-    clocks.start()
     l0 = ens.kernel_launches
-    for k in range(args.steps):
+    for k in range(steps):
         flush.fill_(float(k))
         ev[k][0].record(stream)
         ens.run_fixed(args.dt, 1, use_graph=True)
         ev[k][1].record(stream)
     torch.cuda.synchronize()
     launches = ens.kernel_launches - l0
-    barrier(ws)
-    clk = clocks.stop()
-    ms_total = max_over_ranks(ws, float(sum(a.elapsed_time(b) for a, b in ev)))
-    cells = sum(X * Y * Z for X, Y, Z in dims)
+    ms_total = float(sum(a.elapsed_time(b) for a, b in ev))
+    cells = sum(int(np.prod(dims[i])) for i in mine)
     ens.close()
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
-    if rank != 0:
-        return 0
-    value = args.steps / (ms_total * 1e-3)
-    # roofline of the batched exact potential, the dominant kernel: one FMA per
-    # (target, source) pair of every instance, counting as sources only the
-    # cells whose charge can be non-zero (rho is a central difference of M, so
-    # a cell with a material neighbour), 4 evaluations per RK4 step, over the
-    # whole step's time (a lower bound for the kernel's own rate)
+
     def charge_support(mask):
         m = np.pad(mask != 0, 1)
         sup = np.zeros_like(m)
         for ax in range(3):
             sup |= np.roll(m, 1, axis=ax) | np.roll(m, -1, axis=ax)
         return int(sup[1:-1, 1:-1, 1:-1].sum())
+    # one FMA per (target, source) pair, sources = cells whose charge can be
+    # non-zero (a material neighbour), targets = all cells of the instance
     pairs = float(sum(charge_support(masks[i]) * float(np.prod(dims[i])) for i in mine))
-    fma_peak = mmsb200.fma_tflops()
-    achieved = 4 * 2 * pairs / (ms_total / args.steps * 1e-3) / 1e12
-    roof = {"kernel": "k_ens_direct (batched exact potential)", "bound": "fp32", "unit": "TFLOP/s",
+    return {"steps": steps, "ms_total": ms_total, "cells": cells, "launches": int(launches), "pairs": pairs,
+            "direct_ms": direct_ms, "shape": {"warps": ew, "rows": q}, "instances": len(mine)}
+
+
+def ensemble_summary(args, m, ms_total, ws, fma_peak):
+    value = m["steps"] / (ms_total * 1e-3)
+    achieved = 2 * m["pairs"] / (m["direct_ms"] * 1e-3) / 1e12
+    roof = {"kernel": "k_ens_direct (batched exact potential, persistent)", "bound": "fp32", "unit": "TFLOP/s",
             "achieved": achieved, "peak": fma_peak, "frac": achieved / fma_peak,
             "peak_source": "measured FP32 FMA microbenchmark (mms_diag_fma_tflops), of measured",
-            "algorithmic": "2 flops per target-source pair (sources: cells with a material neighbour; "
-                           "targets: all cells), 4 evaluations per step; timed over the whole step",
-            "traffic": profile_traffic("k_ens_direct_512_instances")}
-    print(json.dumps({"metric": f"ensemble LLG RK4 steps/s ({args.ensemble_size} instances, 16..64 x 16..64 x 3)",
-                      "value": value, "unit": "ensemble steps/s", "n_gpus": ws, "steps": args.steps,
-                      "warmup": max(args.warmup, 3), "ms_per_step": ms_total / args.steps, "higher_is_better": True,
-                      "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-                      "config": {"workload": "ensemble_rk4", "instances": args.ensemble_size, "cells": cells,
-                                 "solver": "direct (batched)", "dt_s": args.dt,
-                                 "l2": "flushed between timed steps", "parallelism": f"instance partition x{ws}"},
-                      "cell_steps_per_s": value * cells, "gpu_launches": int(launches), "clocks": clk,
-                      "roofline": roof}))
+            "algorithmic": "2 flops per target-source pair (sources: cells with a material neighbour; targets: "
+                           "all cells) of every instance, over the kernel's own mean time (CUDA events, "
+                           "back-to-back launches after autotuning)",
+            "kernel_ms": m["direct_ms"], "traffic": profile_traffic("k_ens_direct_512_instances")}
+    return {"metric": f"ensemble LLG RK4 steps/s ({args.ensemble_size} instances, 16..64 x 16..64 x 3)",
+            "value": value, "unit": "ensemble steps/s", "steps": m["steps"], "ms_per_step": ms_total / m["steps"],
+            "cells": m["cells"], "cell_steps_per_s": value * m["cells"], "gpu_launches": m["launches"],
+            "config": {"workload": "ensemble_rk4", "instances": args.ensemble_size, "solver": "direct (batched)",
+                       "dt_s": args.dt, "graph": "one CUDA graph per ensemble step",
+                       "autotuned_shape": m["shape"], "l2": "flushed between timed steps",
+                       "parallelism": f"instance partition x{ws}" if ws > 1 else "single GPU"},
+            "roofline": roof}
+
+
+def run_ensemble(args):
+    """`--workload ensemble`: the batched ensemble alone, as the one JSON line"""
+    import torch
+    import mmsb200
+    ws, rank, local = dist_init()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    clocks = ClockSampler(local)
+    barrier(ws)
+    clocks.start()
+    m = ensemble_measure(args, stream, flush, ws, rank)
+    barrier(ws)
+    clk = clocks.stop()
+    ms_total = max_over_ranks(ws, m["ms_total"])
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = ensemble_summary(args, m, ms_total, ws, mmsb200.fma_tflops())
+    line.update({"n_gpus": ws, "warmup": max(args.warmup, 3), "higher_is_better": True, "scaling": "strong",
+                 "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "clocks": clk})
+    print(json.dumps(line))
     return 0
 
 

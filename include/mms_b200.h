@@ -231,6 +231,11 @@ int64_t mms_ens_kernel_launches(const mms_ens *ens);
 int mms_ens_state_set(mms_ens *ens, const uint8_t *material, const double *M);
 int mms_ens_state_get(mms_ens *ens, double *M, double *t);
 int mms_ens_run_fixed(mms_ens *ens, double dt, int nsteps, int use_graph);
+/* Chooses the batched direct kernel's shape by measurement on the current
+ * state's charges: warps per CTA (4, 8, 16) x source rows staged per batch
+ * (8, 16, 32), `reps` timed launches each; keeps the fastest (the results do
+ * not depend on the shape).  Needs mms_ens_state_set first. */
+int mms_ens_autotune(mms_ens *ens, int reps, int *warps, int *rows, double *best_ms);
 int mms_ens_sync(mms_ens *ens);
 
 /* allocation-free exact potential -------------------------------------------- */

@@ -145,16 +145,23 @@ void drop_graph(mms_ctx *ctx)
 // potential of the state M into ctx->phi
 int eval_state_potential(mms_ctx *ctx, const double *Mst)
 {
+    MmsRange nvtx_("mms/field_evaluation");
     if (!ctx->p.demag) return MMS_OK;  // phi unused
     MMS_TRY(launch_divergence_soa(ctx, Mst, ctx->rho));
     MMS_TRY(launch_potential(ctx, ctx->rho, ctx->phi));
     return MMS_OK;
 }
 
-// one RK4 step on the resident state; phi must hold the potential of M on entry
-// and holds the potential of the new M on exit (4 field evaluations per step)
-int rk4_step_kernels(mms_ctx *ctx)
+// One RK4 step on the resident state, 4 field evaluations.  Normally phi holds
+// the potential of M on entry and of the new M on exit (the k1 field of the
+// next step).  With eval_first the step begins by evaluating the potential of
+// M and leaves the new M's potential unevaluated: a state set from outside
+// (which has no potential yet) then also costs 4 evaluations per step instead
+// of 5.  Both orders evaluate the same potentials of the same states.
+int rk4_step_kernels(mms_ctx *ctx, bool eval_first)
 {
+    MmsRange nvtx_("mms/rk4_step");
+    if (eval_first) MMS_TRY(eval_state_potential(ctx, ctx->M));
     MMS_TRY(launch_rk4_stage(ctx, 0, ctx->M, ctx->A));
     MMS_TRY(eval_state_potential(ctx, ctx->A));
     MMS_TRY(launch_rk4_stage(ctx, 1, ctx->A, ctx->B));
@@ -162,7 +169,7 @@ int rk4_step_kernels(mms_ctx *ctx)
     MMS_TRY(launch_rk4_stage(ctx, 2, ctx->B, ctx->A));
     MMS_TRY(eval_state_potential(ctx, ctx->A));
     MMS_TRY(launch_rk4_stage(ctx, 3, ctx->A, nullptr));
-    MMS_TRY(eval_state_potential(ctx, ctx->M));
+    if (!eval_first) MMS_TRY(eval_state_potential(ctx, ctx->M));
     MMS_TRY(launch_advance_time(ctx));
     return MMS_OK;
 }
@@ -183,19 +190,24 @@ int effective_kind(const mms_ctx *ctx)
     return ctx->s.kind;
 }
 
+// Steps from a state without a potential (set from outside, or parameters
+// changed) run in the evaluate-first order and leave phi invalid; steps from
+// a state with its potential keep it valid.  Either way 4 evaluations a step.
 int run_steps(mms_ctx *ctx, int nsteps, int use_graph)
 {
-    MMS_TRY(ensure_phi(ctx));
+    if (nsteps <= 0) return MMS_OK;
+    const bool ef = !ctx->phi_valid;
     if (!use_graph) {
-        for (int s = 0; s < nsteps; s++) MMS_TRY(rk4_step_kernels(ctx));
+        for (int s = 0; s < nsteps; s++) MMS_TRY(rk4_step_kernels(ctx, ef));
+        ctx->phi_valid = !ef;
         return MMS_OK;
     }
     const int kind = effective_kind(ctx);
-    if (ctx->graph_exec && ctx->graph_solver_kind != kind) drop_graph(ctx);
+    if (ctx->graph_exec && (ctx->graph_solver_kind != kind || ctx->graph_eval_first != ef)) drop_graph(ctx);
     if (!ctx->graph_exec) {
         const int64_t before = ctx->launches;
         MMS_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        int st = rk4_step_kernels(ctx);
+        int st = rk4_step_kernels(ctx, ef);
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
         if (st != MMS_OK) {
@@ -211,17 +223,20 @@ int run_steps(mms_ctx *ctx, int nsteps, int use_graph)
         ctx->graph_kernels = (int)(ctx->launches - before);
         ctx->launches = before;  // captured, not yet launched
         ctx->graph_solver_kind = kind;
+        ctx->graph_eval_first = ef;
     }
     for (int s = 0; s < nsteps; s++) {
         MMS_CUDA_TRY(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
         ctx->launches += ctx->graph_kernels;
     }
+    ctx->phi_valid = !ef;
     return MMS_OK;
 }
 
 // surrogate check on the current state: both potentials, rel-L2, fallback
 int surrogate_check_now(mms_ctx *ctx, double *err_out)
 {
+    MmsRange nvtx_("mms/surrogate_check");
     MMS_TRY(launch_divergence_soa(ctx, ctx->M, ctx->rho));
     float *ps = ctx->vecA, *pf = ctx->vecB;
     MMS_TRY(launch_potential_surrogate(ctx, ctx->rho, ps));
@@ -491,6 +506,7 @@ int mms_divergence_dev(mms_ctx *ctx, const float *M, float *rho)
 
 int mms_potential_dev(mms_ctx *ctx, const float *rho, float *phi)
 {
+    MmsRange nvtx_("mms/potential");
     if (!ctx || !rho || !phi) {
         mms_set_error("NULL argument");
         return MMS_ERR_ARG;
@@ -518,6 +534,7 @@ int mms_exchange_dev(mms_ctx *ctx, const float *M, float *H)
 
 int mms_hfield_dev(mms_ctx *ctx, const float *M, float *H, float *charge, float *potential, double t)
 {
+    MmsRange nvtx_("mms/hfield");
     if (!ctx || !M || !H) {
         mms_set_error("NULL argument");
         return MMS_ERR_ARG;
@@ -574,6 +591,7 @@ int mms_hfield_host(mms_ctx *ctx, const float *M, float *H, float *charge, float
 
 int mms_state_set_dev(mms_ctx *ctx, const uint8_t *material, const double *M, double t)
 {
+    MmsRange nvtx_("mms/state_set_dev");
     if (!ctx || !material || !M) {
         mms_set_error("NULL argument");
         return MMS_ERR_ARG;
@@ -612,6 +630,7 @@ int mms_state_set(mms_ctx *ctx, const uint8_t *material, const double *M, double
 
 int mms_state_get_dev(mms_ctx *ctx, double *M)
 {
+    MmsRange nvtx_("mms/state_get_dev");
     MMS_TRY(require_state(ctx));
     if (!M) {
         mms_set_error("NULL argument");
@@ -645,6 +664,7 @@ int mms_state_get(mms_ctx *ctx, double *M, double *t)
 
 int mms_run_fixed(mms_ctx *ctx, double dt, int nsteps, int use_graph)
 {
+    MmsRange nvtx_("mms/run_fixed");
     MMS_TRY(require_state(ctx));
     if (nsteps < 0 || !(dt > 0) || !isfinite(dt)) {
         mms_set_error("dt must be positive and nsteps >= 0");
@@ -689,6 +709,7 @@ int mms_state_stats(mms_ctx *ctx, double *E_eV, double *torque, double Mavg[3], 
 int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double dt0, mms_record *records,
               int max_records, int *n_records, mms_march_cb cb, void *user)
 {
+    MmsRange nvtx_("mms/march");
     MMS_TRY(require_state(ctx));
     if (!ctl || !(dt0 > 0)) {
         mms_set_error("controller NULL or dt0 <= 0");
@@ -861,6 +882,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
 
 int mms_ctx_set_surrogate(mms_ctx *ctx, const float *w, long long count, int check_every, double tol, int fast)
 {
+    MmsRange nvtx_("mms/set_surrogate");
     if (!ctx || !w || check_every < 0 || !(tol > 0)) {
         mms_set_error("mms_ctx_set_surrogate: bad argument");
         return MMS_ERR_ARG;

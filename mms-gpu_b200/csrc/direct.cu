@@ -214,6 +214,7 @@ int direct_build_table(mms_ctx *ctx)
 
 int launch_potential_direct(mms_ctx *ctx, const float *rho, float *phi)
 {
+    MmsRange nvtx_("mms/direct_potential");
     if (!ctx->gtab) MMS_TRY(direct_build_table(ctx));
     dim3 grid((unsigned)(ctx->g.ydim * ctx->g.zdim), div_up(ctx->g.xdim, SEG));
     k_direct<<<grid, DWARPS * 32, direct_smem_bytes(ctx->g.xdim), ctx->stream>>>(rho, ctx->gtab, phi, ctx->gk());

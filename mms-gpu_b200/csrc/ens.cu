@@ -29,9 +29,9 @@ namespace {
 using namespace mmsdev;
 
 constexpr int ETPB = 256;       // cells per tile / threads per block in the cell kernels
-constexpr int EW = 8;           // warps per CTA in the batched direct kernel
+constexpr int EW_MAX = 16;      // warps per CTA in the batched direct kernel (runtime, autotuned)
 constexpr int ETX = 8;          // targets per lane
-constexpr int QROWS = 16;       // source rows staged per batch
+constexpr int QROWS_MAX = 32;   // source rows staged per batch (runtime, autotuned)
 constexpr int KG = 4;           // source rows summed in FP32 between compensated (Kahan) adds
 
 struct EnsInst {
@@ -91,12 +91,15 @@ __device__ __forceinline__ GridK inst_grid(const EnsInst &in, long long Ntot, do
     return g;
 }
 
+// Persistent cell kernels: an occupancy-sized grid walks the tile table
+// (tile = blockIdx.x, blockIdx.x + gridDim.x, ...).
 __global__ void __launch_bounds__(ETPB) k_ens_div(const double *__restrict__ M, float *__restrict__ rho,
                                                   const EnsInst *__restrict__ inst, const EnsTile *__restrict__ tiles,
-                                                  long long Ntot, double dx, double dy, double dz)
+                                                  int ntiles, long long Ntot, double dx, double dy, double dz)
 {
-    const EnsTile tl = tiles[blockIdx.x];
-    if ((int)threadIdx.x >= tl.count) return;
+  for (int tix = blockIdx.x; tix < ntiles; tix += gridDim.x) {
+    const EnsTile tl = tiles[tix];
+    if ((int)threadIdx.x >= tl.count) continue;
     const EnsInst in = inst[tl.inst];
     const long long i = tl.start + threadIdx.x;
     const long long plane = (long long)in.X * in.Y;
@@ -109,6 +112,7 @@ __global__ void __launch_bounds__(ETPB) k_ens_div(const double *__restrict__ M, 
     const double z2 = (z != in.Z - 1) ? Mz[i + plane] : 0.0;
     const double z0 = (z != 0) ? Mz[i - plane] : 0.0;
     rho[in.off + i] = (float)(0.5 * ((x2 - x0) / dx + (y2 - y0) / dy + (z2 - z0) / dz));
+  }
 }
 
 // one RK4 stage for every instance (see k_rk4_stage in stencil.cu)
@@ -117,11 +121,12 @@ __global__ void __launch_bounds__(ETPB) k_ens_stage(const float *__restrict__ ph
                                                     double *__restrict__ Mnext, const uint8_t *__restrict__ mat,
                                                     const double *__restrict__ tstate, const EnsInst *__restrict__ inst,
                                                     const EnsTile *__restrict__ tiles, double *__restrict__ flag,
-                                                    long long Ntot, double dx, double dy, double dz, PhysK p,
-                                                    int stage)
+                                                    int ntiles, long long Ntot, double dx, double dy, double dz,
+                                                    PhysK p, int stage)
 {
-    const EnsTile tl = tiles[blockIdx.x];
-    if ((int)threadIdx.x >= tl.count) return;
+  for (int tix = blockIdx.x; tix < ntiles; tix += gridDim.x) {
+    const EnsTile tl = tiles[tix];
+    if ((int)threadIdx.x >= tl.count) continue;
     const EnsInst in = inst[tl.inst];
     const long long i = tl.start + threadIdx.x;   // within the instance
     const long long gi = in.off + i;              // global cell
@@ -131,7 +136,7 @@ __global__ void __launch_bounds__(ETPB) k_ens_stage(const float *__restrict__ ph
         dst[gi] = 0.0;
         dst[gi + N] = 0.0;
         dst[gi + 2 * N] = 0.0;
-        return;
+        continue;
     }
     const double dt = tstate[TIME_DT];
     const GridK g = inst_grid(in, Ntot, dx, dy, dz);
@@ -175,6 +180,7 @@ __global__ void __launch_bounds__(ETPB) k_ens_stage(const float *__restrict__ ph
         M[gi + N] = n1;
         M[gi + 2 * N] = n2;
     }
+  }
 }
 
 __global__ void k_ens_advance(double *tstate)
@@ -185,105 +191,121 @@ __global__ void k_ens_advance(double *tstate)
 
 __global__ void k_ens_set_dt(double *tstate, double dt) { tstate[TIME_DT] = dt; }
 
-// batched exact potential (see the file comment)
-__global__ void __launch_bounds__(EW * 32) k_ens_direct(const float *__restrict__ rho, const float *__restrict__ gtab,
-                                                        float *__restrict__ phi, const EnsInst *__restrict__ inst,
-                                                        const EnsDirectItem *__restrict__ items, TableShape t)
+// batched exact potential (see the file comment).  Persistent: an
+// occupancy-sized grid; each CTA stages the mirrored table once, then takes
+// work items (instance, block of target rows) from a shared counter in the
+// order of the item table (costliest first).  blockDim.x / 32 warps per CTA
+// and `qrows` staged source rows per batch are the autotuned shape the items
+// were built for.
+__global__ void __launch_bounds__(EW_MAX * 32) k_ens_direct(const float *__restrict__ rho,
+                                                            const float *__restrict__ gtab, float *__restrict__ phi,
+                                                            const EnsInst *__restrict__ inst,
+                                                            const EnsDirectItem *__restrict__ items, int nitems,
+                                                            unsigned *__restrict__ next, TableShape t, int qrows)
 {
     extern __shared__ __align__(16) float se[];
     const int tsz = t.Z * t.Ym * t.pitch;
     float *gm = se;                       // mirrored table
-    float *qs = se + tsz;                 // [QROWS][Xm] staged source rows
+    float *qs = se + tsz;                 // [qrows][Xm] staged source rows
     for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
         *reinterpret_cast<float4 *>(&gm[i]) = __ldg(reinterpret_cast<const float4 *>(&gtab[i]));
-    const EnsDirectItem it = items[blockIdx.x];
-    const EnsInst in = inst[it.inst];
+    __shared__ int nz[QROWS_MAX];  // staged source row holds a non-zero charge
+    __shared__ int s_item;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r = lane / it.lpr, l = lane % it.lpr;
-    const int nrows = in.Y * in.Z;
-    const int trow = it.row0 + warp * it.rpw + r;
-    const bool active = r < it.rpw && trow < nrows && l * ETX < in.X;
-    const int yt = active ? trow % in.Y : 0, zt = active ? trow / in.Y : 0;
-    const int x0 = l * ETX;
-    const int Xr = (in.X + 7) & ~7;
-    float s[ETX], c[ETX];
+    for (;;) {
+        __syncthreads();  // the previous item is done with the staged rows
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(next, 1u);
+        __syncthreads();
+        const int itx = s_item;
+        if (itx >= nitems) break;
+        const EnsDirectItem it = items[itx];
+        const EnsInst in = inst[it.inst];
+        const int r = lane / it.lpr, l = lane % it.lpr;
+        const int nrows = in.Y * in.Z;
+        const int trow = it.row0 + warp * it.rpw + r;
+        const bool active = r < it.rpw && trow < nrows && l * ETX < in.X;
+        const int yt = active ? trow % in.Y : 0, zt = active ? trow / in.Y : 0;
+        const int x0 = l * ETX;
+        const int Xr = (in.X + 7) & ~7;
+        float s[ETX], c[ETX];
 #pragma unroll
-    for (int i = 0; i < ETX; i++) s[i] = c[i] = 0.f;
-    __shared__ int nz[QROWS];  // staged source row holds a non-zero charge
-    for (int sr0 = 0; sr0 < nrows; sr0 += QROWS) {
-        __syncthreads();
-        if (threadIdx.x < QROWS) nz[threadIdx.x] = 0;
-        __syncthreads();
-        const int nq = min(QROWS, nrows - sr0);
-        for (int i = threadIdx.x; i < QROWS * t.Xm; i += blockDim.x) {
-            const int qr = i / t.Xm, xs = i % t.Xm;
-            const float v = (qr < nq && xs < in.X) ? rho[in.off + (long long)(sr0 + qr) * in.X + xs] : 0.f;
-            qs[i] = v;
-            if (v != 0.f) nz[qr] = 1;  // benign race: every writer stores 1
-        }
-        __syncthreads();
-        if (!active) continue;
-        float acc[ETX];
+        for (int i = 0; i < ETX; i++) s[i] = c[i] = 0.f;
+        for (int sr0 = 0; sr0 < nrows; sr0 += qrows) {
+            __syncthreads();
+            if (threadIdx.x < qrows) nz[threadIdx.x] = 0;
+            __syncthreads();
+            const int nq = min(qrows, nrows - sr0);
+            for (int i = threadIdx.x; i < qrows * t.Xm; i += blockDim.x) {
+                const int qr = i / t.Xm, xs = i % t.Xm;
+                const float v = (qr < nq && xs < in.X) ? rho[in.off + (long long)(sr0 + qr) * in.X + xs] : 0.f;
+                qs[i] = v;
+                if (v != 0.f) nz[qr] = 1;  // benign race: every writer stores 1
+            }
+            __syncthreads();
+            if (!active) continue;
+            float acc[ETX];
 #pragma unroll
-        for (int i = 0; i < ETX; i++) acc[i] = 0.f;
-        for (int qr = 0; qr < nq; qr++) {
-            if (nz[qr]) {  // an all-zero source row adds nothing
-                const int srow = sr0 + qr;
-                const int ys = srow % in.Y, zs = srow / in.Y;
-                const float *grow = gm + (abs(zt - zs) * t.Ym + abs(yt - ys)) * t.pitch;
-                const float *q = qs + qr * t.Xm;
-                // window: win[k] = grow[base + k], base = C - 7 + x0 - xb
-                // C = Xm + 3 with Xm a multiple of 8: base is a multiple of 4, so
-                // the window is read as two 16-byte vectors (a row's lanes are 32 B
-                // apart: at most 2-way bank conflicts instead of 8-way scalar ones)
-                int base = t.C - 7 + x0;
-                float wb[8];
-                {
-                    const float4 u0 = *reinterpret_cast<const float4 *>(grow + base + 8);
-                    const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 12);
-                    wb[0] = u0.x; wb[1] = u0.y; wb[2] = u0.z; wb[3] = u0.w;
-                    wb[4] = u1.x; wb[5] = u1.y; wb[6] = u1.z; wb[7] = u1.w;
-                }
-                for (int xb = 0; xb < Xr; xb += 8) {
-                    float wa[8];
+            for (int i = 0; i < ETX; i++) acc[i] = 0.f;
+            for (int qr = 0; qr < nq; qr++) {
+                if (nz[qr]) {  // an all-zero source row adds nothing
+                    const int srow = sr0 + qr;
+                    const int ys = srow % in.Y, zs = srow / in.Y;
+                    const float *grow = gm + (abs(zt - zs) * t.Ym + abs(yt - ys)) * t.pitch;
+                    const float *q = qs + qr * t.Xm;
+                    // window: win[k] = grow[base + k], base = C - 7 + x0 - xb
+                    // C = Xm + 3 with Xm a multiple of 8: base is a multiple of 4, so
+                    // the window is read as two 16-byte vectors (a row's lanes are 32 B
+                    // apart: at most 2-way bank conflicts instead of 8-way scalar ones)
+                    int base = t.C - 7 + x0;
+                    float wb[8];
                     {
-                        const float4 u0 = *reinterpret_cast<const float4 *>(grow + base);
-                        const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 4);
-                        wa[0] = u0.x; wa[1] = u0.y; wa[2] = u0.z; wa[3] = u0.w;
-                        wa[4] = u1.x; wa[5] = u1.y; wa[6] = u1.z; wa[7] = u1.w;
+                        const float4 u0 = *reinterpret_cast<const float4 *>(grow + base + 8);
+                        const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 12);
+                        wb[0] = u0.x; wb[1] = u0.y; wb[2] = u0.z; wb[3] = u0.w;
+                        wb[4] = u1.x; wb[5] = u1.y; wb[6] = u1.z; wb[7] = u1.w;
                     }
-                    const float4 q0 = *reinterpret_cast<const float4 *>(&q[xb]);
-                    const float4 q1 = *reinterpret_cast<const float4 *>(&q[xb + 4]);
-                    const float qv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-    #pragma unroll
-                    for (int j = 0; j < 8; j++)
-    #pragma unroll
-                        for (int i = 0; i < ETX; i++) {
-                            const int k = 7 + i - j;
-                            acc[i] = fmaf(qv[j], (k < 8) ? wa[k] : wb[k - 8], acc[i]);
+                    for (int xb = 0; xb < Xr; xb += 8) {
+                        float wa[8];
+                        {
+                            const float4 u0 = *reinterpret_cast<const float4 *>(grow + base);
+                            const float4 u1 = *reinterpret_cast<const float4 *>(grow + base + 4);
+                            wa[0] = u0.x; wa[1] = u0.y; wa[2] = u0.z; wa[3] = u0.w;
+                            wa[4] = u1.x; wa[5] = u1.y; wa[6] = u1.z; wa[7] = u1.w;
                         }
-    #pragma unroll
-                    for (int k = 0; k < 8; k++) wb[k] = wa[k];
-                    base -= 8;
-                }
-            }
-            if ((qr + 1) % KG == 0 || qr + 1 == nq) {
+                        const float4 q0 = *reinterpret_cast<const float4 *>(&q[xb]);
+                        const float4 q1 = *reinterpret_cast<const float4 *>(&q[xb + 4]);
+                        const float qv[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
 #pragma unroll
-                for (int i = 0; i < ETX; i++) {  // Kahan across groups of KG source rows
-                    const float y = acc[i] - c[i];
-                    const float tt = s[i] + y;
-                    c[i] = (tt - s[i]) - y;
-                    s[i] = tt;
-                    acc[i] = 0.f;
+                        for (int j = 0; j < 8; j++)
+#pragma unroll
+                            for (int i = 0; i < ETX; i++) {
+                                const int k = 7 + i - j;
+                                acc[i] = fmaf(qv[j], (k < 8) ? wa[k] : wb[k - 8], acc[i]);
+                            }
+#pragma unroll
+                        for (int k = 0; k < 8; k++) wb[k] = wa[k];
+                        base -= 8;
+                    }
+                }
+                if ((qr + 1) % KG == 0 || qr + 1 == nq) {
+#pragma unroll
+                    for (int i = 0; i < ETX; i++) {  // Kahan across groups of KG source rows
+                        const float y = acc[i] - c[i];
+                        const float tt = s[i] + y;
+                        c[i] = (tt - s[i]) - y;
+                        s[i] = tt;
+                        acc[i] = 0.f;
+                    }
                 }
             }
+        }
+        if (active) {
+            float *out = phi + in.off + (long long)trow * in.X;
+#pragma unroll
+            for (int i = 0; i < ETX; i++)
+                if (x0 + i < in.X) out[x0 + i] = s[i] - c[i];
         }
     }
-    if (!active) return;
-    float *out = phi + in.off + (long long)trow * in.X;
-#pragma unroll
-    for (int i = 0; i < ETX; i++)
-        if (x0 + i < in.X) out[x0 + i] = s[i] - c[i];
 }
 
 __global__ void k_aos_to_soa_ens(const double *__restrict__ in, const uint8_t *__restrict__ mat,
@@ -319,6 +341,10 @@ struct mms_ens {
     int ntiles = 0, nitems = 0;
     TableShape ts{};
     size_t direct_smem = 0;
+    int ew = 8, qrows = 16;           // direct-kernel shape (mms_ens_autotune)
+    int grid_direct = 0, grid_cells = 0;
+    unsigned *next = nullptr;         // work counter of the persistent direct kernel
+    std::vector<EnsInst> hin;         // host copy of the offset table
     int64_t launches = 0;
     size_t dev_bytes = 0;
     EnsInst *inst = nullptr;
@@ -375,20 +401,107 @@ int ens_alloc(mms_ens *e, T **p, size_t count)
     return MMS_OK;
 }
 
-int ens_potential(mms_ens *e, const double *Mst)
+// direct-kernel work items for `ew` warps per CTA: (instance, first target
+// row), rpw rows per warp; sorted by decreasing cost (rows x row length x
+// source cells) so that the dynamic schedule ends with the cheapest items
+std::vector<EnsDirectItem> build_items(const std::vector<EnsInst> &hin, int ew)
 {
-    if (!e->p.demag) return MMS_OK;
-    k_ens_div<<<e->ntiles, ETPB, 0, e->stream>>>(Mst, e->rho, e->inst, e->tiles, e->Ntot, e->dx, e->dy, e->dz);
-    ENS_LAUNCH_CHECK(e);
-    k_ens_direct<<<e->nitems, EW * 32, e->direct_smem, e->stream>>>(e->rho, e->gtab, e->phi, e->inst, e->items, e->ts);
+    std::vector<std::pair<double, EnsDirectItem>> v;
+    for (int i = 0; i < (int)hin.size(); i++) {
+        const EnsInst &a = hin[i];
+        const int Xr = (a.X + 7) & ~7;
+        const int lpr = Xr / ETX;                       // lanes per target row (<= 32)
+        const int rpw = std::max(1, 32 / lpr);          // target rows per warp
+        const int nrows = a.Y * a.Z;
+        for (int r0 = 0; r0 < nrows; r0 += rpw * ew) {
+            EnsDirectItem d;
+            d.inst = i;
+            d.row0 = r0;
+            d.rpw = rpw;
+            d.lpr = lpr;
+            const double cost = (double)std::min(rpw * ew, nrows - r0) * Xr * ((double)a.X * a.Y * a.Z);
+            v.push_back({cost, d});
+        }
+    }
+    std::stable_sort(v.begin(), v.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    std::vector<EnsDirectItem> out;
+    for (auto &p : v) out.push_back(p.second);
+    return out;
+}
+
+size_t direct_smem_for(const TableShape &ts, int qrows)
+{
+    return ((size_t)ts.Z * ts.Ym * ts.pitch + (size_t)qrows * ts.Xm) * sizeof(float);
+}
+
+// uploads the item table of shape (ew, qrows) and sizes the persistent grids
+int ens_set_shape(mms_ens *e, int ew, int qrows)
+{
+    const std::vector<EnsDirectItem> items = build_items(e->hin, ew);
+    if ((int)items.size() > e->nitems) {
+        cudaFree(e->items);
+        e->items = nullptr;
+        if (cudaMalloc((void **)&e->items, items.size() * sizeof(EnsDirectItem)) != cudaSuccess) {
+            mms_set_error("ensemble: cudaMalloc of the item table failed");
+            return MMS_ERR_NOMEM;
+        }
+    }
+    e->nitems = (int)items.size();
+    MMS_CUDA_TRY(cudaMemcpyAsync(e->items, items.data(), items.size() * sizeof(EnsDirectItem), cudaMemcpyHostToDevice,
+                                 e->stream));
+    e->ew = ew;
+    e->qrows = qrows;
+    e->direct_smem = direct_smem_for(e->ts, qrows);
+    {
+        // the limit is per kernel and shared by every ensemble: only ever raise it
+        cudaFuncAttributes fa{};
+        MMS_CUDA_TRY(cudaFuncGetAttributes(&fa, k_ens_direct));
+        if ((size_t)fa.maxDynamicSharedSizeBytes < e->direct_smem)
+            MMS_CUDA_TRY(cudaFuncSetAttribute(k_ens_direct, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)e->direct_smem));
+    }
+    int dev = 0, sms = 0, per = 0, perc = 0;
+    MMS_CUDA_TRY(cudaGetDevice(&dev));
+    MMS_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MMS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_ens_direct, ew * 32, e->direct_smem));
+    MMS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perc, k_ens_stage, ETPB, 0));
+    e->grid_direct = std::max(1, std::min(e->nitems, std::max(per, 1) * sms));
+    e->grid_cells = std::max(1, std::min(e->ntiles, std::max(perc, 1) * sms));
+    if (e->exec) {  // a captured step holds the old launch shape
+        cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+    }
+    if (e->graph) {
+        cudaGraphDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    return MMS_OK;
+}
+
+int ens_direct(mms_ens *e)
+{
+    MMS_CUDA_TRY(cudaMemsetAsync(e->next, 0, sizeof(unsigned), e->stream));
+    k_ens_direct<<<e->grid_direct, e->ew * 32, e->direct_smem, e->stream>>>(e->rho, e->gtab, e->phi, e->inst,
+                                                                           e->items, e->nitems, e->next, e->ts,
+                                                                           e->qrows);
     ENS_LAUNCH_CHECK(e);
     return MMS_OK;
 }
 
+int ens_potential(mms_ens *e, const double *Mst)
+{
+    if (!e->p.demag) return MMS_OK;
+    k_ens_div<<<e->grid_cells, ETPB, 0, e->stream>>>(Mst, e->rho, e->inst, e->tiles, e->ntiles, e->Ntot, e->dx, e->dy,
+                                                     e->dz);
+    ENS_LAUNCH_CHECK(e);
+    return ens_direct(e);
+}
+
 int ens_stage(mms_ens *e, int stage, const double *Mst, double *Mnext)
 {
-    k_ens_stage<<<e->ntiles, ETPB, 0, e->stream>>>(e->phi, Mst, e->M, e->K, Mnext, e->mat, e->tstate, e->inst,
-                                                   e->tiles, e->flag, e->Ntot, e->dx, e->dy, e->dz, e->pk(), stage);
+    k_ens_stage<<<e->grid_cells, ETPB, 0, e->stream>>>(e->phi, Mst, e->M, e->K, Mnext, e->mat, e->tstate, e->inst,
+                                                       e->tiles, e->flag, e->ntiles, e->Ntot, e->dx, e->dy, e->dz,
+                                                       e->pk(), stage);
     ENS_LAUNCH_CHECK(e);
     return MMS_OK;
 }
@@ -424,7 +537,6 @@ int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, do
     long long Ntot = 0;
     std::vector<EnsInst> hin(n);
     std::vector<EnsTile> htiles;
-    std::vector<EnsDirectItem> hitems;
     for (int i = 0; i < n; i++) {
         const mms_ens_instance &a = inst[i];
         if (a.xdim < 1 || a.ydim < 1 || a.zdim < 1 || a.xdim > 256) {
@@ -450,17 +562,6 @@ int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, do
             htiles.push_back(t);
         }
         const int Xr = (a.xdim + 7) & ~7;
-        const int lpr = Xr / ETX;                       // lanes per target row (<= 32)
-        const int rpw = std::max(1, 32 / lpr);          // target rows per warp
-        const int nrows = a.ydim * a.zdim;
-        for (int r0 = 0; r0 < nrows; r0 += rpw * EW) {
-            EnsDirectItem d;
-            d.inst = i;
-            d.row0 = r0;
-            d.rpw = rpw;
-            d.lpr = lpr;
-            hitems.push_back(d);
-        }
         Ntot += Ni;
         ts.Xm = std::max(ts.Xm, Xr);
         ts.Ym = std::max(ts.Ym, a.ydim);
@@ -468,7 +569,7 @@ int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, do
     }
     ts.C = ts.Xm + 3;
     ts.pitch = 2 * ts.Xm + 8;
-    const size_t smem = ((size_t)ts.Z * ts.Ym * ts.pitch + (size_t)QROWS * ts.Xm) * sizeof(float);
+    const size_t smem = direct_smem_for(ts, QROWS_MAX);
     if (smem > 200 * 1024) {
         mms_set_error("mms_ens_create: the shared kernel table (%zu B) exceeds 200 KiB; largest instance too big",
                       smem);
@@ -491,9 +592,9 @@ int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, do
         e->p.n_hext = 0;
         e->Ntot = Ntot;
         e->ts = ts;
-        e->direct_smem = smem;
         e->ntiles = (int)htiles.size();
-        e->nitems = (int)hitems.size();
+        e->nitems = 0;
+        e->hin = hin;
         if (stream) {
             e->stream = (cudaStream_t)stream;
         } else {
@@ -507,7 +608,7 @@ int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, do
         const size_t N = (size_t)Ntot;
         if ((st = ens_alloc(e, &e->inst, (size_t)n))) break;
         if ((st = ens_alloc(e, &e->tiles, htiles.size()))) break;
-        if ((st = ens_alloc(e, &e->items, hitems.size()))) break;
+        if ((st = ens_alloc(e, &e->next, 1))) break;
         if ((st = ens_alloc(e, &e->gtab, (size_t)ts.Z * ts.Ym * ts.pitch))) break;
         if ((st = ens_alloc(e, &e->rho, N))) break;
         if ((st = ens_alloc(e, &e->phi, N))) break;
@@ -526,8 +627,6 @@ int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, do
         if (cudaMemcpyAsync(e->inst, hin.data(), n * sizeof(EnsInst), cudaMemcpyHostToDevice, e->stream) ||
             cudaMemcpyAsync(e->tiles, htiles.data(), htiles.size() * sizeof(EnsTile), cudaMemcpyHostToDevice,
                             e->stream) ||
-            cudaMemcpyAsync(e->items, hitems.data(), hitems.size() * sizeof(EnsDirectItem), cudaMemcpyHostToDevice,
-                            e->stream) ||
             cudaMemsetAsync(e->tstate, 0, TIME_SLOTS * sizeof(double), e->stream) ||
             cudaMemsetAsync(e->flag, 0, sizeof(double), e->stream)) {
             mms_set_error("ensemble set-up copies failed");
@@ -536,10 +635,8 @@ int mms_ens_create(const mms_ens_instance *inst, int n, double dx, double dy, do
         }
         const long long tn = (long long)ts.Z * ts.Ym * ts.pitch;
         k_ens_table<<<div_up(tn, 256), 256, 0, e->stream>>>(e->gtab, ts, dx, dy, dz);
-        if (cudaGetLastError() != cudaSuccess ||
-            cudaFuncSetAttribute(k_ens_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                cudaSuccess ||
-            cudaStreamSynchronize(e->stream) != cudaSuccess) {
+        if ((st = ens_set_shape(e, 8, 16))) break;
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(e->stream) != cudaSuccess) {
             mms_set_error("ensemble set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
             st = MMS_ERR_CUDA;
             break;
@@ -564,7 +661,7 @@ int mms_ens_destroy(mms_ens *e)
     if (e->exec) cudaGraphExecDestroy(e->exec);
     if (e->graph) cudaGraphDestroy(e->graph);
     void *b[] = {e->inst, e->tiles, e->items, e->gtab, e->rho, e->phi, e->mat, e->M, e->A, e->B, e->K, e->tstate,
-                 e->flag};
+                 e->flag, e->next};
     for (void *p : b)
         if (p) cudaFree(p);
     if (e->h_scratch) cudaFreeHost(e->h_scratch);
@@ -664,6 +761,55 @@ int mms_ens_run_fixed(mms_ens *e, double dt, int nsteps, int use_graph)
         MMS_CUDA_TRY(cudaGraphLaunch(e->exec, e->stream));
         e->launches += e->graph_kernels;
     }
+    return MMS_OK;
+}
+
+int mms_ens_autotune(mms_ens *e, int reps, int *ew, int *qrows, double *best_ms)
+{
+    if (!e || !e->ready || reps < 1) {
+        mms_set_error("mms_ens_autotune: ensemble state not set or reps < 1");
+        return MMS_ERR_NOT_READY;
+    }
+    // the charges of the current state
+    k_ens_div<<<e->grid_cells, ETPB, 0, e->stream>>>(e->M, e->rho, e->inst, e->tiles, e->ntiles, e->Ntot, e->dx, e->dy,
+                                                     e->dz);
+    ENS_LAUNCH_CHECK(e);
+    cudaEvent_t e0, e1;
+    MMS_CUDA_TRY(cudaEventCreate(&e0));
+    MMS_CUDA_TRY(cudaEventCreate(&e1));
+    const int ews[] = {4, 8, 16}, qs[] = {8, 16, 32};
+    double best = 1e30;
+    int bew = e->ew, bq = e->qrows, st = MMS_OK;
+    for (int a : ews)
+        for (int q : qs) {
+            if (st != MMS_OK) break;
+            if ((st = ens_set_shape(e, a, q))) break;
+            if ((st = ens_direct(e))) break;  // warm
+            cudaEventRecord(e0, e->stream);
+            for (int r = 0; r < reps && st == MMS_OK; r++) st = ens_direct(e);
+            cudaEventRecord(e1, e->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) {
+                mms_set_error("mms_ens_autotune: %s", cudaGetErrorString(cudaGetLastError()));
+                st = MMS_ERR_CUDA;
+                break;
+            }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms / reps < best) {
+                best = ms / reps;
+                bew = a;
+                bq = q;
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MMS_TRY(st);
+    MMS_TRY(ens_set_shape(e, bew, bq));
+    e->phi_valid = false;
+    MMS_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (ew) *ew = bew;
+    if (qrows) *qrows = bq;
+    if (best_ms) *best_ms = best;
     return MMS_OK;
 }
 

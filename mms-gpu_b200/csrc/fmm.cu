@@ -2586,6 +2586,7 @@ int fmm_far_error(mms_ctx *ctx)
 
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
 {
+    MmsRange nvtx_("mms/fmm_potential");
     FmmPlan *pl = ctx->fmm;
     if (!pl) {
         mms_set_error("FMM plan missing");
@@ -2992,6 +2993,7 @@ int farnet_bind(mms_ctx *ctx, const float *w, long long count)
 // three launches on the main one; the last adds the two
 int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
 {
+    MmsRange nvtx_("mms/surrogate_potential");
     FmmPlan *pl = ctx->fmm;
     if (!pl || !pl->fn_ready) {
         mms_set_error("surrogate solver: no weights bound (mms_ctx_set_surrogate)");

@@ -8,6 +8,17 @@
 #include <vector>
 
 #include "mms_b200.h"
+#include <nvtx3/nvToolsExt.h>
+
+// NVTX range over a scope (host side): names the public entry points and the
+// stages of a field evaluation in a profiler's timeline (nsys, or ncu
+// --nvtx --nvtx-include "mms/..."); free when no profiler is attached.
+struct MmsRange {
+    explicit MmsRange(const char *name) { nvtxRangePushA(name); }
+    ~MmsRange() { nvtxRangePop(); }
+    MmsRange(const MmsRange &) = delete;
+    MmsRange &operator=(const MmsRange &) = delete;
+};
 
 // ---------------------------------------------------------------------------
 // error plumbing: every failure becomes a status code and a thread-local message
@@ -116,6 +127,7 @@ struct mms_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_kernels = 0;
     int graph_solver_kind = -1;
+    bool graph_eval_first = false;              // the captured step evaluates phi(M) first
 
     GridK gk() const {
         GridK k;

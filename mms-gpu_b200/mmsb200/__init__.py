@@ -120,6 +120,7 @@ SIGNATURES = {
     "mms_ens_state_get": (_I, [_VP, _VP, ctypes.POINTER(_D)]),
     "mms_ens_run_fixed": (_I, [_VP, _D, _I, _I]),
     "mms_ens_sync": (_I, [_VP]),
+    "mms_ens_autotune": (_I, [_VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D)]),
     "mms_fmm_stage_times": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_D)]),
     "mms_farnet_num_params": (ctypes.c_longlong, []),
     "mms_farnet_create": (_I, [_I, _I, _I, ctypes.POINTER(_VP)]),

@@ -115,3 +115,10 @@ class Ensemble:
 
     def sync(self):
         _check(load().mms_ens_sync(self.h))
+
+    def autotune(self, reps=5):
+        """measured shape of the batched direct kernel: (warps per CTA, source
+        rows per batch, ms per potential)"""
+        w, q, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(load().mms_ens_autotune(self.h, reps, ctypes.byref(w), ctypes.byref(q), ctypes.byref(ms)))
+        return w.value, q.value, ms.value

@@ -97,34 +97,39 @@ def generate_pairs(n_pairs, X=256, Y=256, Z=3, snaps_per_run=50, steps_between=1
     F = torch.empty_like(U)
     N2 = torch.empty(n_pairs, dtype=torch.float32, device="cuda")
     grid = Grid(X, Y, Z, DX, DX, DX)
-    dyn = Context(grid, make_params(), make_solver(SOLVER_FMM, 4, LEAF))
-    tgt = Context(grid, make_params(), make_solver(SOLVER_FMM, target_order, LEAF))
+    # one stream for both contexts and for the torch copies: the charges the
+    # dynamics context writes are read by the target context in order
+    st = torch.cuda.Stream()
+    dyn = Context(grid, make_params(), make_solver(SOLVER_FMM, 4, LEAF), stream=st.cuda_stream)
+    tgt = Context(grid, make_params(), make_solver(SOLVER_FMM, target_order, LEAF), stream=st.cuda_stream)
     Mdev = torch.empty((N, 3), dtype=torch.float64, device="cuda")
     rho = torch.empty(N, dtype=torch.float32, device="cuda")
     phi = torch.empty_like(rho)
     near = torch.empty_like(rho)
     k = 0
     t0 = time.time()
+    torch.cuda.synchronize()
     try:
-        while k < n_pairs:
-            mask, M = _place(*_instance(rng, Z), X, Y, rng)
-            ht, hb = _field(rng)
-            dyn.set_params(make_params(external=True, hext_t=ht, hext_b=hb))
-            dyn.state_set(mask, M)
-            for s in range(snaps_per_run):
-                if k >= n_pairs:
-                    break
-                if s:
-                    dyn.run_fixed(dt, steps_between)
-                dyn.state_get_dev(Mdev)
-                dyn.divergence_dev(Mdev.float(), rho)
-                tgt.potential_split_dev(rho, phi, near)
-                U[k] = (rho * (DX / MS)).view(Z, Y, X)
-                F[k] = ((phi - near) / (MS * DX)).view(Z, Y, X)
-                N2[k] = ((phi / (MS * DX)).double() ** 2).sum().float()
-                k += 1
-            if progress:
-                progress(k, time.time() - t0)
+        with torch.cuda.stream(st):
+            while k < n_pairs:
+                mask, M = _place(*_instance(rng, Z), X, Y, rng)
+                ht, hb = _field(rng)
+                dyn.set_params(make_params(external=True, hext_t=ht, hext_b=hb))
+                dyn.state_set(mask, M)
+                for s in range(snaps_per_run):
+                    if k >= n_pairs:
+                        break
+                    if s:
+                        dyn.run_fixed(dt, steps_between)
+                    dyn.state_get_dev(Mdev)
+                    dyn.divergence_dev(Mdev.float(), rho)
+                    tgt.potential_split_dev(rho, phi, near)
+                    U[k] = (rho * (DX / MS)).view(Z, Y, X)
+                    F[k] = ((phi - near) / (MS * DX)).view(Z, Y, X)
+                    N2[k] = ((phi / (MS * DX)).double() ** 2).sum().float()
+                    k += 1
+                if progress:
+                    progress(k, time.time() - t0)
         torch.cuda.synchronize()
     finally:
         dyn.close()
@@ -148,8 +153,10 @@ def benchmark_pairs(n_pairs, seed=777, X=256, Y=256, Z=3, steps_between=20, dt=1
     phi = torch.empty_like(rho)
     near = torch.empty_like(rho)
     prm = make_params(external=True, hext_t=[0.0, 1e-8], hext_b=[[-0.05, 0, 0], [0.05, 0, 0]])
-    with Context(grid, prm, make_solver(SOLVER_FMM, 4, LEAF)) as dyn, \
-            Context(grid, make_params(), make_solver(SOLVER_FMM, 8, LEAF)) as tgt:
+    st = torch.cuda.Stream()  # one stream for both contexts and the torch copies
+    torch.cuda.synchronize()
+    with torch.cuda.stream(st), Context(grid, prm, make_solver(SOLVER_FMM, 4, LEAF), stream=st.cuda_stream) as dyn, \
+            Context(grid, make_params(), make_solver(SOLVER_FMM, 8, LEAF), stream=st.cuda_stream) as tgt:
         per_run = 10
         for k in range(n_pairs):
             if k % per_run == 0:
@@ -163,6 +170,7 @@ def benchmark_pairs(n_pairs, seed=777, X=256, Y=256, Z=3, steps_between=20, dt=1
             U[k] = (rho * (DX / MS)).view(Z, Y, X)
             F[k] = ((phi - near) / (MS * DX)).view(Z, Y, X)
             P[k] = (phi / (MS * DX)).view(Z, Y, X)
+        torch.cuda.synchronize()
     N2 = (P.double() ** 2).flatten(1).sum(1).float()
     return U, F, N2, P
 

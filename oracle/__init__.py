@@ -49,9 +49,11 @@ class _Params(ctypes.Structure):
 
 
 def build(quiet: bool = True) -> None:
-    """Compile liboracle.so and, when the reference tree is present, the
-    reference harness (``make -C oracle``)."""
-    out = subprocess.run(["make", "-C", HERE, "all"], capture_output=True, text=True)
+    """Compile liboracle.so and, when the reference tree is present (its path
+    in MMS_REFERENCE_TREE, else the reference's location in the build
+    container), the reference harness (``make -C oracle REF=...``)."""
+    ref = os.environ.get("MMS_REFERENCE_TREE", "/root/reference")
+    out = subprocess.run(["make", "-C", HERE, "all", f"REF={ref}"], capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
