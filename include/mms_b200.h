@@ -316,6 +316,10 @@ int mms_farnet_forward_dev(mms_farnet *net, const float *u, float *out, int nbat
  * device [nbatch][3][Y][X]; nrm2: device [nbatch] */
 int mms_farnet_gradient(mms_farnet *net, const float *u, const float *far, const float *nrm2, int nbatch,
                         float *grad, double *loss);
+/* per-weight multipliers of the Adam step (host array of num_params; 1 each
+ * at creation): a weight moves by lr * scale_i per unit of normalised
+ * gradient, e.g. scale_i ~ |w_i| for relative steps */
+int mms_farnet_set_step_scale(mms_farnet *net, const float *scale, long long count);
 /* one Adam step on that loss; *loss is the loss before the step */
 int mms_farnet_train_step(mms_farnet *net, const float *u, const float *far, const float *nrm2, int nbatch,
                           float lr, float beta1, float beta2, float eps, double *loss);

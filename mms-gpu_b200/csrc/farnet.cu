@@ -36,12 +36,13 @@ struct mms_farnet {
     long long lev_off[FN_DEPTHS + 3] = {};
     long long *lev_dev = nullptr;
     float *w = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;  // weights, gradient, Adam moments
+    float *sc = nullptr;  // per-weight step scale (1 unless set)
     float *M = nullptr, *Lf = nullptr, *dM = nullptr, *dL = nullptr;
     float *out = nullptr, *dout = nullptr;
     double *lsum = nullptr;
     bf16 *A = nullptr, *B = nullptr;
-    float *Cm = nullptr;
-    size_t a_elems = 0, b_elems = 0, c_elems = 0;
+    float *Cm = nullptr, *Cp = nullptr;  // GEMM result, split-K partials
+    size_t a_elems = 0, b_elems = 0, c_elems = 0, p_elems = 0;
     long long step = 0;
     size_t bytes = 0;
 };
@@ -396,9 +397,12 @@ __global__ void k_t_scatter(const float *__restrict__ C, int fam, int d, int nb_
     }
 }
 
+// Adam with a per-weight step scale: a weight moves by lr * sc_i per unit of
+// normalised gradient, so tables whose entries span many orders of magnitude
+// take relative steps
 __global__ void k_t_adam(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
-                         float *__restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
-                         float c2)
+                         float *__restrict__ v, const float *__restrict__ sc, long long n, float lr, float b1,
+                         float b2, float eps, float c1, float c2)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -407,7 +411,13 @@ __global__ void k_t_adam(float *__restrict__ w, const float *__restrict__ g, flo
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] -= lr * sc[i] * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void k_t_fill(float *__restrict__ a, long long n, float v)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
 }
 
 NetK netk(const mms_farnet *n, int nbatch)
@@ -458,8 +468,14 @@ int gemm_family(mms_farnet *n, const NetK &k, GatherP p, int fa, int fb, int d, 
     k_t_gather<<<nblk((long long)fa * p.Kp), TB>>>(pa, k, n->A);
     k_t_gather<<<nblk((long long)fb * p.Kp), TB>>>(pb, k, n->B);
     MMS_CUDA_TRY(cudaGetLastError());
-    const int K3 = (int)(3 * p.Kp);
-    MMS_TRY(umma_gemm_bf16(n->A, K3, n->B, K3, n->Cm, fb, fa, fb, K3, 0, fb <= 64 ? 64 : 128, 0));
+    const int K3 = (int)(3 * p.Kp), bn = fb <= 64 ? 64 : 128;
+    int splits = 1, kchunk = K3;
+    MMS_TRY(umma_gemm_bf16_splitk_plan(fa, fb, K3, bn, &splits, &kchunk));
+    if ((size_t)splits * fa * fb > n->p_elems) {
+        mms_set_error("farnet: split-K partial buffer too small");
+        return MMS_ERR_ARG;
+    }
+    MMS_TRY(umma_gemm_bf16_splitk(n->A, K3, n->B, K3, n->Cm, n->Cp, fa, fb, K3, bn, splits, kchunk, 0));
     const int ops = p.fam == FAM_M2L ? 49 : 4;
     const int cnt = (p.fam == FAM_W || p.fam == FAM_V) ? FN_C * FN_NR : ops * FN_OSZ;
     k_t_scatter<<<nblk(cnt), TB>>>(n->Cm, p.fam, d, ops, n->g);
@@ -572,10 +588,12 @@ int mms_farnet_create(int xdim, int ydim, int batch, mms_farnet **out)
     n->a_elems = (size_t)(49 * FN_NR * 3 * Kp);  // A: up to max(49 NR, C) features
     n->b_elems = (size_t)(4 * FN_NR * 3 * Kp);
     n->c_elems = (size_t)49 * FN_NR * FN_NR + (size_t)FN_C * FN_NR;
+    n->p_elems = n->c_elems * 148;  // up to one split per SM
     struct {
         void **p;
         size_t bytes;
     } a[] = {{(void **)&n->w, P * sizeof(float)},
+             {(void **)&n->sc, P * sizeof(float)},
              {(void **)&n->g, P * sizeof(float)},
              {(void **)&n->m, P * sizeof(float)},
              {(void **)&n->v, P * sizeof(float)},
@@ -589,6 +607,7 @@ int mms_farnet_create(int xdim, int ydim, int batch, mms_farnet **out)
              {(void **)&n->A, n->a_elems * sizeof(bf16)},
              {(void **)&n->B, std::max(n->b_elems, (size_t)(FN_C * 3 * Kp)) * sizeof(bf16)},
              {(void **)&n->Cm, n->c_elems * sizeof(float)},
+             {(void **)&n->Cp, n->c_elems * 148 * sizeof(float)},
              {(void **)&n->lev_dev, (FN_DEPTHS + 3) * sizeof(long long)}};
     n->b_elems = std::max(n->b_elems, (size_t)(FN_C * 3 * Kp));  // B: up to max(4 NR, C) features
     for (auto &e : a) {
@@ -600,6 +619,7 @@ int mms_farnet_create(int xdim, int ydim, int batch, mms_farnet **out)
         n->bytes += e.bytes;
     }
     cudaMemset(n->w, 0, P * sizeof(float));
+    k_t_fill<<<nblk(P), TB>>>(n->sc, P, 1.f);
     cudaMemset(n->m, 0, P * sizeof(float));
     cudaMemset(n->v, 0, P * sizeof(float));
     if (cudaMemcpy(n->lev_dev, n->lev_off, sizeof(n->lev_off), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -615,7 +635,7 @@ void mms_farnet_destroy(mms_farnet *n)
 {
     if (!n) return;
     cudaDeviceSynchronize();
-    void *b[] = {n->w, n->g, n->m, n->v, n->M, n->Lf, n->dM, n->dL, n->out, n->dout, n->lsum, n->A, n->B, n->Cm,
+    void *b[] = {n->w, n->sc, n->g, n->m, n->v, n->M, n->Lf, n->dM, n->dL, n->out, n->dout, n->lsum, n->A, n->B, n->Cm, n->Cp,
                  n->lev_dev};
     for (void *p : b)
         if (p) cudaFree(p);
@@ -632,6 +652,16 @@ int mms_farnet_set_weights(mms_farnet *n, const float *w, long long count)
     MMS_CUDA_TRY(cudaMemset(n->m, 0, count * sizeof(float)));
     MMS_CUDA_TRY(cudaMemset(n->v, 0, count * sizeof(float)));
     n->step = 0;
+    return MMS_OK;
+}
+
+int mms_farnet_set_step_scale(mms_farnet *n, const float *scale, long long count)
+{
+    if (!n || !scale || count != fn_num_params()) {
+        mms_set_error("mms_farnet_set_step_scale: need %lld scales", fn_num_params());
+        return MMS_ERR_ARG;
+    }
+    MMS_CUDA_TRY(cudaMemcpy(n->sc, scale, count * sizeof(float), cudaMemcpyHostToDevice));
     return MMS_OK;
 }
 
@@ -683,7 +713,7 @@ int mms_farnet_train_step(mms_farnet *n, const float *u, const float *far, const
     n->step++;
     const float c1 = 1.f - powf(beta1, (float)n->step), c2 = 1.f - powf(beta2, (float)n->step);
     const long long P = fn_num_params();
-    k_t_adam<<<nblk(P), TB>>>(n->w, n->g, n->m, n->v, P, lr, beta1, beta2, eps, c1, c2);
+    k_t_adam<<<nblk(P), TB>>>(n->w, n->g, n->m, n->v, n->sc, P, lr, beta1, beta2, eps, c1, c2);
     MMS_CUDA_TRY(cudaGetLastError());
     return MMS_OK;
 }

@@ -2637,6 +2637,7 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
 constexpr int FN_UP_THREADS = 384;
 constexpr int FN_DOWN_THREADS = 256;
 constexpr int FN_WP = FN_C + 4;  // encoder row pitch in shared memory (floats)
+constexpr int FN_DN_CELLS = (FN_Z * 16 * 16 + FN_DOWN_THREADS - 1) / FN_DOWN_THREADS;  // cells per thread in k_fn_down
 
 namespace {
 
@@ -2809,14 +2810,45 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
     __shared__ float cur[FN_NR], nxt[FN_NR], leaf[4][FN_NR];
     extern __shared__ __align__(16) float dsm[];
     const int L = f.L;
+    // the near field of this CTA's cells, every load issued before anything waits
+    int nlx0, nly0, nrw;
+    if (L <= 2) {
+        nlx0 = blockIdx.x % (1 << L);
+        nly0 = blockIdx.x / (1 << L);
+        nrw = FN_S;
+    } else {
+        nlx0 = 2 * (blockIdx.x % (1 << (L - 1)));
+        nly0 = 2 * (blockIdx.x / (1 << (L - 1)));
+        nrw = 2 * FN_S;
+    }
+    float nv[FN_DN_CELLS];
+#pragma unroll
+    for (int r = 0; r < FN_DN_CELLS; r++) {
+        const int e = threadIdx.x + r * FN_DOWN_THREADS;
+        const int rx = e % nrw, ry = (e / nrw) % nrw, lz = e / (nrw * nrw);
+        const int x = nlx0 * FN_S + rx, y = nly0 * FN_S + ry;
+        float v = 0.f;
+        if (e < FN_Z * nrw * nrw && x < f.X && y < f.Y) {
+            const long long cell = ((long long)lz * f.Y + y) * f.X + x;
+            v = __ldg(&near[cell]);
+            for (int qn = 1; qn < nnear; qn++) v += __ldg(&near[qn * near_stride + cell]);
+        }
+        nv[r] = v;
+    }
     float *Vs = dsm;                  // [NR][C]
-    float *Ts = Vs + FN_NR * FN_C;    // L2L tables of parent levels 2 .. L-1
-    float *Lc = Ts + (L > 2 ? (L - 2) * 4 * FN_OSZ : 0);  // interaction-list locals: ancestors 2..L-1, 4 leaves
-    fn_stage(Vs, V, FN_NR * FN_C);
-    if (L > 2) fn_stage(Ts, Tl2l, (L - 2) * 4 * FN_OSZ);
+    // L2L tables the chain uses: for levels 3 .. L-1 the one of the CTA's
+    // ancestor's child position, then the 4 of level L-1 (the leaves')
+    float *Ts = Vs + FN_NR * FN_C;
+    float *Lc = Ts + (L > 2 ? (L + 1) * FN_OSZ : 0);  // interaction-list locals: ancestors 2..L-1, 4 leaves
     if (L > 2) {
-        // the CTA's chain, every load in flight at once: level l (2..L-1) ancestor, then the 4 leaves
         const int np = 1 << (L - 1), pbx = blockIdx.x % np, pby = blockIdx.x / np;
+        for (int l = 3; l <= L - 1; l++) {
+            const int sh = L - 1 - l, bx = pbx >> sh, by = pby >> sh;
+            const int c = (by & 1) * 2 + (bx & 1);
+            fn_stage(Ts + (l - 3) * FN_OSZ, Tl2l + ((long long)(l - 1 - 2) * 4 + c) * FN_OSZ, FN_OSZ);
+        }
+        fn_stage(Ts + (L - 3) * FN_OSZ, Tl2l + (long long)(L - 1 - 2) * 4 * FN_OSZ, 4 * FN_OSZ);
+        // the CTA's chain, every load in flight at once: level l (2..L-1) ancestor, then the 4 leaves
         for (int i = threadIdx.x; i < (L + 2) * (FN_NR / 4); i += blockDim.x) {
             const int r = i / (FN_NR / 4), k4 = i % (FN_NR / 4);
             long long box;
@@ -2831,7 +2863,9 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    fn_stage(Vs, V, FN_NR * FN_C);  // a second group: the decoder, needed only after the chain
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     __syncthreads();
     int nlf, lx0, ly0;  // leaves handled and the first one
     if (L <= 2) {
@@ -2848,9 +2882,7 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) cur[k] = Lc[k];
         __syncthreads();
         for (int l = 3; l <= L - 1; l++) {
-            const int sh = L - 1 - l, bx = pbx >> sh, by = pby >> sh;
-            const int c = (by & 1) * 2 + (bx & 1);
-            const float *T = Ts + ((l - 1 - 2) * 4 + c) * FN_OSZ;
+            const float *T = Ts + (l - 3) * FN_OSZ;
             for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) nxt[k] = Lc[(l - 2) * FN_NR + k] + fn_apply(T, cur, k);
             __syncthreads();
             for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) cur[k] = nxt[k];
@@ -2861,27 +2893,33 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         nlf = 4;
         for (int i = threadIdx.x; i < 4 * FN_NR; i += blockDim.x) {
             const int c = i / FN_NR, k = i % FN_NR;
-            const float *T = Ts + ((L - 1 - 2) * 4 + c) * FN_OSZ;
+            const float *T = Ts + (L - 3 + c) * FN_OSZ;
             leaf[c][k] = Lc[(L - 2 + c) * FN_NR + k] + fn_apply(T, cur, k);
         }
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
-    // decoder + near field over the region, a row at a time
+    // decoder + near field over the region, a row at a time; the near field
+    // (complete before the launch) was read into registers at the start
     const int gw = nlf == 4 ? 2 : 1, rw = gw * FN_S;
-    for (int e = threadIdx.x; e < FN_Z * rw * rw; e += blockDim.x) {
+#pragma unroll
+    for (int r = 0; r < FN_DN_CELLS; r++) {
+        const int e = threadIdx.x + r * FN_DOWN_THREADS;
+        if (e >= FN_Z * rw * rw) break;
         const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
         const int x = lx0 * FN_S + rx, y = ly0 * FN_S + ry;
         if (x >= f.X || y >= f.Y) continue;
         const long long cell = ((long long)lz * f.Y + y) * f.X + x;
         const int b = (ry / FN_S) * gw + rx / FN_S, c = lz * FN_S * FN_S + (ry % FN_S) * FN_S + rx % FN_S;
-        float acc = __ldg(&near[cell]);
-        for (int qn = 1; qn < nnear; qn++) acc += __ldg(&near[qn * near_stride + cell]);
+        float acc = nv[r];
         const float *lb = leaf[b];
 #pragma unroll 8
         for (int k = 0; k < FN_NR; k++) acc = fmaf(Vs[k * FN_C + c], lb[k], acc);
         phi[cell] = acc;
     }
 }
+
+int fn_up_level(int L) { return std::max(2, L - 2); }
 
 size_t fn_up_smem(int L)
 {
@@ -2894,8 +2932,7 @@ size_t fn_up_smem(int L)
 
 size_t fn_down_smem(int L)
 {
-    return ((size_t)FN_NR * FN_C + (size_t)std::max(L - 2, 0) * 4 * FN_OSZ + (size_t)(L + 2) * FN_NR) *
-           sizeof(float);
+    return ((size_t)FN_NR * FN_C + (size_t)(L > 2 ? L + 1 : 0) * FN_OSZ + (size_t)(L + 2) * FN_NR) * sizeof(float);
 }
 
 }  // namespace
@@ -3014,7 +3051,7 @@ int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
         MMS_LAUNCH_CHECK(ctx);
         return MMS_OK;
     }
-    const int cb = std::max(2, f.L - 2);
+    const int cb = fn_up_level(f.L);
     MMS_CUDA_TRY(launch_k(k_fn_up, dim3(1u << (2 * cb)), dim3(FN_UP_THREADS), fn_up_smem(f.L), ctx->stream, rho,
                           (const float *)pl->fnW, (const float *)pl->fnM2M, pl->fnM, (const long long *)pl->lev_dev,
                           pl->fnCtr, f, cb));

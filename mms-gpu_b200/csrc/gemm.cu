@@ -1,5 +1,7 @@
 // BF16 tensor-core GEMM entry points on the tcgen05 core (umma.cuh):
 // C = A B^T or C += A B^T with A (M x K) and B (N x K) K-major.
+#include <algorithm>
+
 #include "mms_internal.cuh"
 #include "umma.cuh"
 
@@ -17,6 +19,32 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const __nv_bfloat16 *__restri
     umma::Smem<BN> &s = *reinterpret_cast<umma::Smem<BN> *>(base);
     umma::gemm_tile<BN>(A, lda, B, ldb, C, ldc, M, N, K, blockIdx.x * umma::BM, blockIdx.y * BN, beta, &g_umma_err,
                         s);
+}
+
+// split-K: CTA (m tile, n tile, split s) multiplies the K range
+// [s kchunk, (s + 1) kchunk) into its own partial C (Cp + s M N, beta 0)
+template <int BN>
+__global__ void __launch_bounds__(128) k_gemm_bf16_splitk(const __nv_bfloat16 *__restrict__ A, int lda,
+                                                          const __nv_bfloat16 *__restrict__ B, int ldb,
+                                                          float *__restrict__ Cp, int M, int N, int K, int kchunk)
+{
+    extern __shared__ uint8_t raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+    umma::Smem<BN> &s = *reinterpret_cast<umma::Smem<BN> *>(base);
+    const int k0 = blockIdx.z * kchunk;
+    const int kn = min(kchunk, K - k0);
+    umma::gemm_tile<BN>(A + k0, lda, B + k0, ldb, Cp + (size_t)blockIdx.z * M * N, N, M, N, kn, blockIdx.x * umma::BM,
+                        blockIdx.y * BN, 0, &g_umma_err, s);
+}
+
+// C = sum of the splits' partials, in split order
+__global__ void k_splitk_reduce(const float *__restrict__ Cp, int splits, long long MN, float *__restrict__ C)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= MN) return;
+    float v = Cp[i];
+    for (int s = 1; s < splits; s++) v += Cp[(long long)s * MN + i];
+    C[i] = v;
 }
 
 template <int BN>
@@ -55,6 +83,52 @@ int umma_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C, int
         mms_set_error("gemm: tile N must be 64 or 128");
         return MMS_ERR_ARG;
     }
+}
+
+int umma_gemm_bf16_splitk_plan(int M, int N, int K, int bn, int *splits, int *kchunk)
+{
+    const int tiles = (int)(div_up(M, umma::BM) * div_up(N, bn));
+    int sp = std::max(1, std::min(148 / std::max(tiles, 1), (K + 63) / 64));
+    int kc = ((K + sp - 1) / sp + 63) / 64 * 64;
+    sp = (K + kc - 1) / kc;
+    *splits = sp;
+    *kchunk = kc;
+    return MMS_OK;
+}
+
+int umma_gemm_bf16_splitk(const void *A, int lda, const void *B, int ldb, float *C, float *Cpart, int M, int N,
+                          int K, int bn, int splits, int kchunk, cudaStream_t st)
+{
+    if (M < 1 || N < 1 || K < 8 || (K % 8) || (lda % 8) || (ldb % 8) || lda < K || ldb < K || kchunk % 64 ||
+        (long long)splits * kchunk < K || (long long)(splits - 1) * kchunk >= K) {
+        mms_set_error("gemm split-K: bad shape");
+        return MMS_ERR_ARG;
+    }
+    // the two tile widths have the same function type: one set-up flag each
+    static bool attr64 = false, attr128 = false;
+    auto launch = [&](auto kern, size_t smem, bool &attr) -> int {
+        if (!attr) {
+            MMS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            attr = true;
+        }
+        dim3 grid(div_up(M, umma::BM), div_up(N, bn), splits);
+        kern<<<grid, 128, smem, st>>>((const __nv_bfloat16 *)A, lda, (const __nv_bfloat16 *)B, ldb, Cpart, M, N, K,
+                                      kchunk);
+        MMS_CUDA_TRY(cudaGetLastError());
+        return MMS_OK;
+    };
+    if (bn == 64)
+        MMS_TRY(launch(k_gemm_bf16_splitk<64>, gemm_smem<64>(), attr64));
+    else if (bn == 128)
+        MMS_TRY(launch(k_gemm_bf16_splitk<128>, gemm_smem<128>(), attr128));
+    else {
+        mms_set_error("gemm split-K: tile N must be 64 or 128");
+        return MMS_ERR_ARG;
+    }
+    const long long MN = (long long)M * N;
+    k_splitk_reduce<<<div_up(MN, 256), 256, 0, st>>>(Cpart, splits, MN, C);
+    MMS_CUDA_TRY(cudaGetLastError());
+    return MMS_OK;
 }
 
 int umma_check_error()

@@ -175,6 +175,12 @@ size_t fmm_plan_bytes(const mms_ctx *ctx);
 // tcgen05 BF16 GEMM (gemm.cu): C (+)= A B^T, A M x K, B N x K, K-major
 int umma_gemm_bf16(const void *A, int lda, const void *B, int ldb, float *C, int ldc, int M, int N, int K, int beta,
                    int bn, cudaStream_t st);
+// split-K form for long K and few output tiles: `splits` CTAs per tile, each
+// over kchunk (a multiple of 64) of K into Cpart[splits][M][N], then C = the
+// fixed-order sum; umma_gemm_bf16_splitk_plan picks splits for ~one wave
+int umma_gemm_bf16_splitk_plan(int M, int N, int K, int bn, int *splits, int *kchunk);
+int umma_gemm_bf16_splitk(const void *A, int lda, const void *B, int ldb, float *C, float *Cpart, int M, int N,
+                          int K, int bn, int splits, int kchunk, cudaStream_t st);
 int umma_check_error();
 
 // potential with the context's solver

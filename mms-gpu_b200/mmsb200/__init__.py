@@ -127,6 +127,7 @@ SIGNATURES = {
     "mms_farnet_destroy": (None, [_VP]),
     "mms_farnet_set_weights": (_I, [_VP, _VP, ctypes.c_longlong]),
     "mms_farnet_get_weights": (_I, [_VP, _VP, ctypes.c_longlong]),
+    "mms_farnet_set_step_scale": (_I, [_VP, _VP, ctypes.c_longlong]),
     "mms_farnet_forward_dev": (_I, [_VP, _VP, _VP, _I]),
     "mms_farnet_gradient": (_I, [_VP, _VP, _VP, _VP, _I, _VP, ctypes.POINTER(_D)]),
     "mms_farnet_train_step": (_I, [_VP, _VP, _VP, _VP, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -463,6 +464,10 @@ class FarNet:
         w = np.empty(self.num_params(), np.float32)
         _check(load().mms_farnet_get_weights(self.h, _ptr(w), w.size))
         return w
+
+    def set_step_scale(self, scale):
+        s = np.ascontiguousarray(scale, np.float32)
+        _check(load().mms_farnet_set_step_scale(self.h, _ptr(s), s.size))
 
     def forward_dev(self, u, out, nbatch=1):
         _check(load().mms_farnet_forward_dev(self.h, _ptr(u), _ptr(out), nbatch))

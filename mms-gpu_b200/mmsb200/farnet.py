@@ -187,3 +187,24 @@ def h2_init(depths=DEPTHS, R=8, Rup=4):
         w[off[("M2M", d)]:off[("M2M", d)] + 4 * OSZ] = m2m.ravel()
         w[off[("L2L", d)]:off[("L2L", d)] + 4 * OSZ] = l2l.ravel()
     return w
+
+
+def step_scale(w, floor=1e-3, depths=DEPTHS):
+    """per-weight Adam step scale for relative updates: |w_i| plus a floor of
+    `floor` x the largest magnitude of w_i's table, so that entries that are
+    zero can still move (the near-field M2L slots get 0: they never enter)"""
+    w = np.asarray(w, np.float64)
+    off = layout(depths)
+    s = np.abs(w)
+    keys = ["W", "V"] + [("M2L", d) for d in range(depths)] + [(n, d) for d in range(1, depths)
+                                                                 for n in ("M2M", "L2L")]
+    starts = sorted(off[k] for k in keys) + [off["total"]]
+    for a, b in zip(starts[:-1], starts[1:]):
+        s[a:b] += floor * np.abs(w[a:b]).max()
+    for d in range(depths):
+        base = off[("M2L", d)]
+        for oy in (-1, 0, 1):
+            for ox in (-1, 0, 1):
+                o = base + slot(ox, oy) * OSZ
+                s[o:o + OSZ] = 0.0
+    return s.astype(np.float32)

@@ -34,11 +34,13 @@ DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "farnet_w24_d5.npz")
 
 # ---- training geometries ------------------------------------------------------
 
-def _instance(rng, Z):
-    """(mask, M) of one instance with sides drawn from 64..256"""
+def _instance(rng, Z, kinds=None):
+    """(mask, M) of one instance with sides drawn from 64..256; kinds: the
+    geometry kinds to draw from (0, 1 disc lattices; 2 disc or ellipse; 3
+    rectangle; 4 block-masked film; 5 vortex-quadrant square), all when None"""
     sides = (64, 96, 128, 160, 192, 224, 256)
     sx, sy = int(rng.choice(sides)), int(rng.choice(sides))
-    kind = int(rng.integers(0, 6))
+    kind = int(rng.integers(0, 6)) if kinds is None else int(rng.choice(kinds))
     seed = int(rng.integers(0, 2 ** 31))
     if kind in (0, 1):  # disc lattice (the benchmark's family)
         r = int(rng.integers(5, 17))
@@ -87,7 +89,7 @@ def _field(rng):
 
 
 def generate_pairs(n_pairs, X=256, Y=256, Z=3, snaps_per_run=50, steps_between=10, dt=1e-13, seed=2010,
-                   target_order=8, progress=None):
+                   target_order=8, progress=None, kinds=None):
     """n_pairs training pairs: torch tensors U, F [n, Z, Y, X] and N2 [n]
     (float32, cuda)"""
     import torch
@@ -112,7 +114,7 @@ def generate_pairs(n_pairs, X=256, Y=256, Z=3, snaps_per_run=50, steps_between=1
     try:
         with torch.cuda.stream(st):
             while k < n_pairs:
-                mask, M = _place(*_instance(rng, Z), X, Y, rng)
+                mask, M = _place(*_instance(rng, Z, kinds), X, Y, rng)
                 ht, hb = _field(rng)
                 dyn.set_params(make_params(external=True, hext_t=ht, hext_b=hb))
                 dyn.state_set(mask, M)
@@ -191,16 +193,19 @@ def evaluate(net, U, F, N2, P=None, batch=8):
     return dict(total_mean=float(np.mean(et)), total_max=float(np.max(et)))
 
 
-def train(U, F, N2, steps, batch=8, lr_max=3e-5, lr_min=3e-7, warmup=0.02, seed=1, weights=None, val=None,
+def train(U, F, N2, steps, batch=8, lr_max=1e-4, lr_min=1e-6, warmup=0.02, seed=1, weights=None, val=None,
           log_every=250, log=print):
     """fits the network (from `weights`, else the nested-SVD start) to the
-    pairs with Adam on a warm-up + cosine schedule; returns (weights, history,
-    start weights); with `val`, the weights of the best validation mean"""
+    pairs with Adam on a warm-up + cosine schedule; steps are relative to
+    each weight's magnitude (farnet.step_scale), so lr is a relative step;
+    returns (weights, history, start weights); with `val`, the weights of the
+    best validation mean"""
     import torch
     Z, Y, X = U.shape[1:]
     net = FarNet(X, Y, batch)
     w0 = np.asarray(farnet.h2_init() if weights is None else weights, np.float32)
     net.set_weights(w0)
+    net.set_step_scale(farnet.step_scale(w0))
     g = torch.Generator(device="cpu").manual_seed(seed)
     hist = []
     t0 = time.time()
@@ -270,7 +275,7 @@ def main(argv=None):
     ap.add_argument("--pairs", type=int, default=4000)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=8)
-    ap.add_argument("--lr", type=float, default=3e-5)
+    ap.add_argument("--lr", type=float, default=1e-4, help="peak relative step")
     ap.add_argument("--val", type=int, default=40)
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--log", default=None)
