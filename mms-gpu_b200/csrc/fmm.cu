@@ -273,7 +273,6 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
                                                  float *__restrict__ Mall, long long off_leaf, FmmDev f, int wsm,
                                                  int up, const float *__restrict__ Tm2m, long long off_par)
 {
-    pdl_begin();
     extern __shared__ __align__(16) float q[];
     const int rows = up ? 2 : 1;
     const int NE = f.NE, NO = f.NR - f.NE, s = f.s, CB = f.C * PB;
@@ -293,6 +292,9 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
         for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4)
             umma::cp_async16(umma::smem_u32(Ts + i), Tm2m + i, true);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
+    // weights and operators are constant and already in flight; the charges
+    // are the predecessor's output
+    pdl_begin();
     const int bx0 = blockIdx.x * PB, by0 = rows * blockIdx.y;
     {
         const int RW = PB * s, nrow = rows * f.Z * s;
@@ -609,16 +611,17 @@ __global__ void __maxnreg__(NR_ <= 30 ? 112 : 255) k_m2l_res(const float *__rest
                                                             const long long *__restrict__ lev_off, FmmDev f,
                                                             long long lstride)
 {
-    pdl_begin();
     constexpr int NO_ = NR_ - NE_;
     constexpr int OSZ = NE_ * NE_ + NO_ * NO_;
     extern __shared__ __align__(16) float sr[];
     Tc += (long long)(items[blockIdx.x].x - 2) * lstride;
     // stage the operator table with asynchronous copies: every 16-byte chunk
-    // in flight at once instead of one load-store round trip per chunk
+    // in flight at once instead of one load-store round trip per chunk; the
+    // table is constant, so it streams in while the predecessor finishes
     for (int i = threadIdx.x * 4; i < 49 * OSZ; i += blockDim.x * 4)
         umma::cp_async16(umma::smem_u32(&sr[i]), &Tc[i], true);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
+    pdl_begin();
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     (void)f;
     m2l_res_item<NR_, NE_, true>(Mall, Lout, sr, sr, items[blockIdx.x], lev_off);
@@ -672,7 +675,6 @@ __device__ __forceinline__ void l2l_top_box(float *__restrict__ Lfin, const floa
 __global__ void __launch_bounds__(512) k_top_m2m(float *__restrict__ Mall, const float *__restrict__ Tb,
                                                  long long off2, long long off3, long long off4, FmmDev f)
 {
-    pdl_begin();
     extern __shared__ __align__(16) float smb[];
     const int NE = f.NE, NO = f.NR - f.NE;
     const int tsz = 4 * (NE * NE + NO * NO);
@@ -683,7 +685,9 @@ __global__ void __launch_bounds__(512) k_top_m2m(float *__restrict__ Mall, const
     float *G = Ts + tsz + 4 * (4 * f.NR + 4 * KT);  // [4][NR]: the level-3 children, child index = grp
     const int P = blockIdx.x;
     const int cx = 2 * (P % 4) + (grp & 1), cy = 2 * (P / 4) + (grp >> 1);
+    // the operators are constant: they stream in while the predecessor finishes
     for (int i = threadIdx.x * 4; i < tsz; i += blockDim.x * 4) umma::cp_async16(umma::smem_u32(Ts + i), Tb + i, true);
+    pdl_begin();
     for (int i = t; i < 4 * f.NR; i += 4 * KT) {  // the group's four level-4 children
         const int c = i / f.NR, j = i % f.NR;
         cp_async4(Mc + i, Mall + (off4 + (long long)(2 * cy + (c >> 1)) * 16 + 2 * cx + (c & 1)) * f.NR + j, true);
@@ -890,7 +894,6 @@ template <int S, int BB, int G>
 __global__ void __launch_bounds__(512) k_p2p(const float *__restrict__ rho, const float *__restrict__ Gn,
                                               float *__restrict__ out, FmmDev f)
 {
-    pdl_begin();
     extern __shared__ __align__(16) float sl[];
     const int Z = f.Z;
     constexpr int W = (BB + 2) * S;        // charges per staged row
@@ -1012,7 +1015,6 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
                                               int nnear, long long near_stride, const float *__restrict__ Lpart_all,
                                               const long long *__restrict__ lev_off)
 {
-    pdl_begin();
     extern __shared__ __align__(16) float sl[];
     const int Z = f.Z;
     const int NE = f.NE, NO = f.NR - f.NE;
@@ -1035,6 +1037,7 @@ __global__ void __launch_bounds__(512) k_l2p(const float *__restrict__ near, con
             umma::cp_async16(umma::smem_u32(Ts + i), Tl2l + i, true);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
+    pdl_begin();  // the operators above are constant; what follows is the predecessors' output
     float ppre, lpre;  // partial 0 of this thread's first parent and leaf item
     // pmode 4: partial 0 of this thread's ancestor item at levels 2 .. 4 (the
     // item the level loop below gives it when GB NR <= blockDim)
@@ -2680,7 +2683,6 @@ __global__ void __launch_bounds__(FN_UP_THREADS) k_fn_up(const float *__restrict
                                                          const long long *__restrict__ lev_off,
                                                          unsigned *__restrict__ ctr, FmmDev f, int cb)
 {
-    pdl_begin();
     extern __shared__ __align__(16) float fsm[];
     const int gs = 1 << (f.L - cb), G = gs * gs, ncb = 1 << cb;
     const int cbx = blockIdx.x % ncb, cby = blockIdx.x / ncb;  // the CTA's box at level cb
@@ -2696,6 +2698,7 @@ __global__ void __launch_bounds__(FN_UP_THREADS) k_fn_up(const float *__restrict
     }
     fn_stage(Ts, Tm2m, (f.L - 2) * 4 * FN_OSZ);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
+    pdl_begin();  // the weights above are constant; the charges are the predecessor's output
     // charges, a region row at a time (consecutive threads on consecutive x);
     // every load of a thread is issued before the first store
     const int rw = gs * FN_S, ne = FN_Z * rw * rw;
@@ -2806,10 +2809,29 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
                                                              long long near_stride, float *__restrict__ phi,
                                                              const long long *__restrict__ lev_off, FmmDev f)
 {
-    pdl_begin();
     __shared__ float cur[FN_NR], nxt[FN_NR], leaf[4][FN_NR];
     extern __shared__ __align__(16) float dsm[];
     const int L = f.L;
+    float *Vs = dsm;                  // [NR][C]
+    // L2L tables the chain uses: for levels 3 .. L-1 the one of the CTA's
+    // ancestor's child position, then the 4 of level L-1 (the leaves'); they
+    // and the decoder are constant, so they stream in while the predecessors
+    // finish (group 0: tables, group 1: decoder)
+    float *Ts = Vs + FN_NR * FN_C;
+    float *Lc = Ts + (L > 2 ? (L + 1) * FN_OSZ : 0);  // interaction-list locals: ancestors 2..L-1, 4 leaves
+    if (L > 2) {
+        const int np = 1 << (L - 1), pbx = blockIdx.x % np, pby = blockIdx.x / np;
+        for (int l = 3; l <= L - 1; l++) {
+            const int sh = L - 1 - l, bx = pbx >> sh, by = pby >> sh;
+            const int c = (by & 1) * 2 + (bx & 1);
+            fn_stage(Ts + (l - 3) * FN_OSZ, Tl2l + ((long long)(l - 1 - 2) * 4 + c) * FN_OSZ, FN_OSZ);
+        }
+        fn_stage(Ts + (L - 3) * FN_OSZ, Tl2l + (long long)(L - 1 - 2) * 4 * FN_OSZ, 4 * FN_OSZ);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    fn_stage(Vs, V, FN_NR * FN_C);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    pdl_begin();
     // the near field of this CTA's cells, every load issued before anything waits
     int nlx0, nly0, nrw;
     if (L <= 2) {
@@ -2835,19 +2857,8 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         }
         nv[r] = v;
     }
-    float *Vs = dsm;                  // [NR][C]
-    // L2L tables the chain uses: for levels 3 .. L-1 the one of the CTA's
-    // ancestor's child position, then the 4 of level L-1 (the leaves')
-    float *Ts = Vs + FN_NR * FN_C;
-    float *Lc = Ts + (L > 2 ? (L + 1) * FN_OSZ : 0);  // interaction-list locals: ancestors 2..L-1, 4 leaves
     if (L > 2) {
         const int np = 1 << (L - 1), pbx = blockIdx.x % np, pby = blockIdx.x / np;
-        for (int l = 3; l <= L - 1; l++) {
-            const int sh = L - 1 - l, bx = pbx >> sh, by = pby >> sh;
-            const int c = (by & 1) * 2 + (bx & 1);
-            fn_stage(Ts + (l - 3) * FN_OSZ, Tl2l + ((long long)(l - 1 - 2) * 4 + c) * FN_OSZ, FN_OSZ);
-        }
-        fn_stage(Ts + (L - 3) * FN_OSZ, Tl2l + (long long)(L - 1 - 2) * 4 * FN_OSZ, 4 * FN_OSZ);
         // the CTA's chain, every load in flight at once: level l (2..L-1) ancestor, then the 4 leaves
         for (int i = threadIdx.x; i < (L + 2) * (FN_NR / 4); i += blockDim.x) {
             const int r = i / (FN_NR / 4), k4 = i % (FN_NR / 4);
@@ -2862,10 +2873,8 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
             umma::cp_async16(umma::smem_u32(Lc + r * FN_NR + 4 * k4), Lp + box * FN_NR + 4 * k4, true);
         }
     }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    fn_stage(Vs, V, FN_NR * FN_C);  // a second group: the decoder, needed only after the chain
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");  // group 2: the chain
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     int nlf, lx0, ly0;  // leaves handled and the first one
     if (L <= 2) {
@@ -2897,7 +2906,6 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
             leaf[c][k] = Lc[(L - 2 + c) * FN_NR + k] + fn_apply(T, cur, k);
         }
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     // decoder + near field over the region, a row at a time; the near field
     // (complete before the launch) was read into registers at the start
