@@ -444,8 +444,10 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
     """The learned far field on the same workload: its demag error on the start
     state against the exact sum, LLG steps/s with the network alone (no
     check), and the surrogate-assisted run the metric names (FMM check every
-    50 steps, 1e-3 rel-L2 tolerance, FMM takes over above it), each as K
-    graph-replayed steps timed with CUDA events on the library's stream."""
+    50 steps, 1e-3 rel-L2 tolerance, FMM takes over above it), and the FMM at
+    P = 5 and 6 (the orders whose error brackets the network's) with their
+    errors, each as K graph-replayed steps timed with CUDA events on the
+    library's stream."""
     import torch
     import mmsb200
     from mmsb200 import farnet
@@ -474,13 +476,14 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
             dctx.sync()
         out["demag_phi_rel_l2_vs_direct"] = float((phi_s.double() - phi_d.double()).norm() / phi_d.double().norm())
 
-    def steps_per_s(every, tol, nsteps):
-        with mmsb200.Context(grid, params, solver, stream=stream.cuda_stream) as c:
-            c.set_surrogate(w, every, tol)
+    def steps_per_s(every, tol, nsteps, slv=solver):
+        with mmsb200.Context(grid, params, slv, stream=stream.cuda_stream) as c:
+            if every is not None:
+                c.set_surrogate(w, every, tol)
             c.state_set(mask, M)
             c.run_fixed(args.dt, 3)
             c.sync()
-            st0 = c.surrogate_stats()
+            st0 = c.surrogate_stats() if every is not None else None
             ms = 0.0
             for k in range(nsteps):
                 flush.fill_(float(k))
@@ -490,6 +493,8 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
                 e1.record(stream)
                 torch.cuda.synchronize()
                 ms += e0.elapsed_time(e1)
+            if every is None:
+                return nsteps / (ms * 1e-3), None
             st = c.surrogate_stats()
             st["checks"] -= st0["checks"]
             return nsteps / (ms * 1e-3), st
@@ -503,6 +508,20 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
                                        "fallbacks": st["fallbacks"], "max_check_rel_l2_vs_fmm": st["max_err"],
                                        "surrogate_active_at_end": st["active"],
                                        "speedup_vs_fmm": v / fmm_value}
+    # the FMM at the orders that bracket the network's accuracy, on the same
+    # state and steps: what the network is worth at equal error
+    matched = []
+    for P in (5, 6):
+        slv = mmsb200.make_solver(mmsb200.SOLVER_FMM, P, 8)
+        with mmsb200.Context(grid, params, slv, stream=stream.cuda_stream) as c:
+            phi_f = torch.empty_like(rho)
+            c.potential_dev(rho, phi_f)
+            c.sync()
+            err = float((phi_f.double() - phi_d.double()).norm() / phi_d.double().norm())
+        v, _ = steps_per_s(None, None, n, slv)
+        matched.append({"P": P, "leaf": 8, "demag_phi_rel_l2_vs_direct": err, "steps_per_s": v,
+                        "network_speedup": out["steps_per_s_surrogate_only"] / v})
+    out["fmm_at_matched_accuracy"] = matched
     return out
 
 

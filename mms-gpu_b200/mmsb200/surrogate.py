@@ -266,12 +266,59 @@ def load_weights(path=DEFAULT_WEIGHTS):
         return z["weights"].astype(np.float32), meta
 
 
+def time_potential(evals=50, X=256, Y=256, Z=3, seed=9100, order=4, weights=None):
+    """one potential evaluation of the network (exact near field + learned far
+    field) against the FMM at `order` (leaf 8) on a state of the benchmark
+    workload (disc lattice, per-dot random in-plane M): mean time over
+    `evals` back-to-back evaluations (CUDA events on the contexts' stream,
+    after 5 untimed), and each one's rel-L2 error against the exact sum;
+    the network runs first, then the FMM"""
+    import torch
+    from . import SOLVER_DIRECT, SOLVER_SURROGATE
+    w = weights if weights is not None else load_weights()[0]
+    if w is None:
+        raise RuntimeError("network weights missing")
+    grid = Grid(X, Y, Z, DX, DX, DX)
+    mask, M = geometry.per_dot_random_inplane(X, Y, Z, 12, 32, seed)
+    st = torch.cuda.Stream()
+    out = {}
+    with torch.cuda.stream(st):
+        rho = torch.empty(X * Y * Z, dtype=torch.float32, device="cuda")
+        ref = torch.empty_like(rho)
+        with Context(grid, make_params(), make_solver(SOLVER_DIRECT), stream=st.cuda_stream) as d:
+            d.divergence_dev(torch.from_numpy(M.astype(np.float32)).cuda(), rho)
+            d.potential_dev(rho, ref)
+            d.sync()
+        for name, slv in (("network", make_solver(SOLVER_SURROGATE, 6, LEAF)),
+                          ("fmm", make_solver(SOLVER_FMM, order, LEAF))):
+            with Context(grid, make_params(), slv, stream=st.cuda_stream) as c:
+                if name == "network":
+                    c.set_surrogate(w, 0, 1.0)
+                phi = torch.empty_like(rho)
+                for _ in range(5):
+                    c.potential_dev(rho, phi)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                for _ in range(evals):
+                    c.potential_dev(rho, phi)
+                e1.record(st)
+                c.sync()
+                torch.cuda.synchronize()
+                out[name] = {"us": e0.elapsed_time(e1) * 1e3 / evals,
+                             "rel_l2_vs_direct": float((phi.double() - ref.double()).norm() / ref.double().norm())}
+    out["fmm"]["order"] = order
+    return out
+
+
 def main(argv=None):
     import argparse
     import json
 
     import torch
-    ap = argparse.ArgumentParser(description="train the learned far-field network")
+    ap = argparse.ArgumentParser(description="train the learned far-field network, or time it against the FMM")
+    ap.add_argument("--time", action="store_true",
+                    help="time one potential evaluation, network vs FMM, on the benchmark workload, and exit")
+    ap.add_argument("--evals", type=int, default=50, help="evaluations timed with --time")
     ap.add_argument("--pairs", type=int, default=4000)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=8)
@@ -280,6 +327,9 @@ def main(argv=None):
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--log", default=None)
     a = ap.parse_args(argv)
+    if a.time:
+        print(json.dumps(time_potential(a.evals)), flush=True)
+        return
     logf = open(a.log, "w") if a.log else None
 
     def log(rec):

@@ -315,3 +315,20 @@ def test_march_checks_on_rejected_steps(cuda, lib, tol, stays):
     assert st == mmsb200.MMS_OK and abs(t - 2e-12) < 1e-24
     assert s["checks"] >= 1
     assert s["active"] == stays and s["fallbacks"] == (0 if stays else 1)
+
+
+def test_time_potential_cli(cuda, lib):
+    """python -m mmsb200.surrogate --time: one JSON line with the network's and
+    the FMM's potential time and error on the benchmark workload"""
+    import json
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ)
+    env["PYTHONPATH"] = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "mms-gpu_b200")
+    r = subprocess.run([sys.executable, "-m", "mmsb200.surrogate", "--time", "--evals", "10"], env=env,
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d["network"]["rel_l2_vs_direct"] < 1e-4 < d["fmm"]["rel_l2_vs_direct"] < 1e-3
+    assert d["network"]["us"] > 0 and d["fmm"]["us"] > 0
