@@ -135,7 +135,7 @@ def test_c4_512_instances_5000_steps(cuda, lib):
     5000 graph-replayed steps of dt = 1e-13 s.  Every instance keeps |M| = Ms
     and stays finite, and one instance of each mask kind (the largest of its
     kind) ends within 0.1 deg of an independent single-grid context run the
-    same 5000 steps."""
+    same 5000 steps (measured: 6e-6 deg; bound 1e-3 deg)."""
     import mmsb200
     from mmsb200 import geometry
     from mmsb200.ensemble import Ensemble
@@ -164,5 +164,5 @@ def test_c4_512_instances_5000_steps(cuda, lib):
             ref_ctx, _ = ctx.state_get()
         a = max_angle_deg(out[i], ref_ctx, masks[i])
         worst = max(worst, a)
-        assert a < 0.1, (i, dims[i], a)
+        assert a < 1e-3, (i, dims[i], a)
     print(f"C4 5000 steps: max angle vs single contexts {worst:.2e} deg")
