@@ -134,7 +134,7 @@ def test_c4_512_instances_5000_steps(cuda, lib):
     """The batched-ensemble configuration at its full length: 512 instances,
     5000 graph-replayed steps of dt = 1e-13 s.  Every instance keeps |M| = Ms
     and stays finite, and one instance of each mask kind (the largest of its
-    kind) ends within 0.1 deg of an independent single-grid context run the
+    kind) ends within 1e-3 deg of an independent single-grid context run the
     same 5000 steps (measured: 6e-6 deg; bound 1e-3 deg)."""
     import mmsb200
     from mmsb200 import geometry
