@@ -699,6 +699,185 @@ __global__ void __launch_bounds__(512) k_top_m2m(float *__restrict__ Mall, const
     m2m_reduce(Mall, Ts, G, red, off2, P, f, t, KT, grp == 0);
 }
 
+// ---- upward pass in one launch (leaf side 8, 3 layers) ----------------------
+// The learned far field's encoder and upward pass (NR_ channels, NE_ of them
+// even).  The FMM's own P2M + M2M launches stay separate: at P = 4 this one
+// launch of 64 CTAs measured 10.9 us in the RK4 step against 10.6 us for
+// k_p2m_row (128 CTAs) + k_top_m2m under programmatic launch.
+constexpr int UP_THREADS = 384;
+constexpr int UP_S = 8, UP_Z = 3, UP_C = UP_S * UP_S * UP_Z;  // leaf box: 8 x 8 cells x 3 layers
+constexpr int UP_WP = UP_C + 4;  // weight row pitch in shared memory (floats): conflict-free 16-byte reads
+
+// one output k of a block-diagonal map: sum_j T[blk][j][k] x[j], T one
+// operator [even NE_ x NE_ | odd NO x NO] input-major, in the order of
+// m2m_reduce's per-child sums
+template <int NR_, int NE_>
+__device__ __forceinline__ float blk_apply(const float *T, const float *x, int k)
+{
+    constexpr int NO_ = NR_ - NE_;
+    if (k < NE_) {
+        float acc = 0.f;
+#pragma unroll
+        for (int j = 0; j < NE_; j++) acc = fmaf(T[j * NE_ + k], x[j], acc);
+        return acc;
+    }
+    const int kk = k - NE_;
+    const float *To = T + NE_ * NE_;
+    float acc = 0.f;
+#pragma unroll
+    for (int j = 0; j < NO_; j++) acc = fmaf(To[j * NO_ + kk], x[NE_ + j], acc);
+    return acc;
+}
+
+// Leaf multipoles and the whole upward pass.  CTA = one box of level cb =
+// max(2, L - 2), i.e. gs x gs leaf boxes (gs = 2^(L - cb) <= 4): their
+// charges and the weights W ([NR][C], k-major) are staged in shared memory,
+// the leaf multipoles (p2m_dot's four interleaved chains, so the same bits)
+// and every level up to cb formed there and written out.  Levels above cb:
+// the CTA that completes the fourth child of a box forms that box (an
+// arrival counter per box in ctr, reset by that CTA for the next launch;
+// writers fence their stores before they arrive, the last arriver fences
+// before it reads the siblings through L2), and so on up to level 2.  No CTA
+// waits for another.  M2M sums the four children as m2m_reduce does,
+// (c0 + c1) + (c2 + c3).  tls: floats between the M2M tables of consecutive
+// levels (0: one table for every level).
+template <int NR_, int NE_>
+__global__ void __launch_bounds__(UP_THREADS) k_up(const float *__restrict__ rho, const float *__restrict__ W,
+                                                   const float *__restrict__ Tm2m, long long tls,
+                                                   float *__restrict__ Mall, const long long *__restrict__ lev_off,
+                                                   unsigned *__restrict__ ctr, FmmDev f, int cb)
+{
+    constexpr int OSZ = NE_ * NE_ + (NR_ - NE_) * (NR_ - NE_);
+    extern __shared__ __align__(16) float usm[];
+    const int gs = 1 << (f.L - cb), G = gs * gs, ncb = 1 << cb;
+    const int cbx = blockIdx.x % ncb, cby = blockIdx.x / ncb;  // the CTA's box at level cb
+    const int bx0 = cbx * gs, by0 = cby * gs;                  // its first leaf box
+    const int ntab = tls ? f.L - 2 : 1;
+    float *Ws = usm;                       // [NR][UP_WP]: weight rows, padded
+    float *Ts = Ws + NR_ * UP_WP;          // M2M tables: [ntab][4][OSZ]
+    float *q = Ts + ntab * 4 * OSZ;        // [G][C]
+    float *mb = q + G * UP_C;              // multipoles of levels L .. cb, G NR + G/4 NR + ...
+    __shared__ int s_last;
+    for (int i = threadIdx.x; i < NR_ * UP_C / 4; i += blockDim.x) {
+        const int k = i / (UP_C / 4), c4 = i % (UP_C / 4);
+        umma::cp_async16(umma::smem_u32(Ws + k * UP_WP + 4 * c4), W + k * UP_C + 4 * c4, true);
+    }
+    for (int i = threadIdx.x * 4; i < ntab * 4 * OSZ; i += blockDim.x * 4)
+        umma::cp_async16(umma::smem_u32(Ts + i), Tm2m + i, true);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    pdl_begin();  // the weights above are constant; the charges are the predecessor's output
+    // charges, a region row at a time (consecutive threads on consecutive x);
+    // every load of a thread is issued before the first store
+    const int rw = gs * UP_S, ne = UP_Z * rw * rw;
+    constexpr int QR = (UP_Z * 32 * 32 + UP_THREADS - 1) / UP_THREADS;
+    float qv[QR];
+#pragma unroll
+    for (int r = 0; r < QR; r++) {
+        const int e = threadIdx.x + r * blockDim.x;
+        const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
+        const int x = bx0 * UP_S + rx, y = by0 * UP_S + ry;
+        qv[r] = (e < ne && x < f.X && y < f.Y) ? __ldg(&rho[((long long)lz * f.Y + y) * f.X + x]) : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < QR; r++) {
+        const int e = threadIdx.x + r * blockDim.x;
+        if (e >= ne) break;
+        const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
+        const int b = (ry / UP_S) * gs + rx / UP_S, c = lz * UP_S * UP_S + (ry % UP_S) * UP_S + rx % UP_S;
+        q[b * UP_C + c] = qv[r];
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    // leaf multipoles: four interleaved chains per output (p2m_dot's order)
+    const long long offL = lev_off[f.L];
+    for (int o = threadIdx.x; o < G * NR_; o += blockDim.x) {
+        const int b = o / NR_, k = o % NR_;
+        const float4 *qb = reinterpret_cast<const float4 *>(q + b * UP_C);
+        const float4 *wk = reinterpret_cast<const float4 *>(Ws + k * UP_WP);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll 8
+        for (int c4 = 0; c4 < UP_C / 4; c4++) {
+            const float4 wv = wk[c4], qv4 = qb[c4];
+            a0 = fmaf(wv.x, qv4.x, a0);
+            a1 = fmaf(wv.y, qv4.y, a1);
+            a2 = fmaf(wv.z, qv4.z, a2);
+            a3 = fmaf(wv.w, qv4.w, a3);
+        }
+        const float v = (a0 + a1) + (a2 + a3);
+        mb[o] = v;
+        const int bx = bx0 + b % gs, by = by0 + b / gs;
+        Mall[(offL + (long long)by * f.nb + bx) * NR_ + k] = v;
+    }
+    __syncthreads();
+    // levels L-1 .. cb inside the CTA
+    const float *child = mb;
+    float *par = mb + G * NR_;
+    int gc = gs;
+    for (int l = f.L - 1; l >= cb; l--) {
+        const int gp = gc / 2, n = 1 << l;
+        const float *T = Ts + (tls ? (l - 2) : 0) * 4 * OSZ;
+        const int px0 = bx0 >> (f.L - l), py0 = by0 >> (f.L - l);
+        for (int o = threadIdx.x; o < gp * gp * NR_; o += blockDim.x) {
+            const int p = o / NR_, k = o % NR_, px = p % gp, py = p / gp;
+            float a[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                a[c] = blk_apply<NR_, NE_>(T + c * OSZ, child + ((2 * py + (c >> 1)) * gc + 2 * px + (c & 1)) * NR_, k);
+            const float v = (a[0] + a[1]) + (a[2] + a[3]);
+            par[o] = v;
+            Mall[(lev_off[l] + (long long)(py0 + py) * n + px0 + px) * NR_ + k] = v;
+        }
+        __syncthreads();
+        child = par;
+        par += gp * gp * NR_;
+        gc = gp;
+    }
+    // levels above cb: the last of four siblings to finish forms the parent
+    int bxl = cbx, byl = cby;
+    for (int l = cb - 1; l >= 2; l--) {
+        __threadfence();  // this CTA's multipoles are visible before it arrives
+        __syncthreads();
+        const int px = bxl >> 1, py = byl >> 1, n = 1 << l, nc = 2 * n;
+        if (threadIdx.x == 0) {
+            const unsigned t = atomicAdd(&ctr[lev_off[l] + (long long)py * n + px], 1u);
+            s_last = t == 3;
+        }
+        __syncthreads();
+        if (!s_last) return;
+        __threadfence();
+        float *sib = mb;  // the four children, read through L2
+        for (int i = threadIdx.x; i < 4 * NR_; i += blockDim.x) {
+            const int c = i / NR_, k = i % NR_;
+            sib[i] = __ldcg(&Mall[(lev_off[l + 1] + (long long)(2 * py + (c >> 1)) * nc + 2 * px + (c & 1)) * NR_ + k]);
+        }
+        __syncthreads();
+        const float *T = Ts + (tls ? (l - 2) : 0) * 4 * OSZ;
+        for (int k = threadIdx.x; k < NR_; k += blockDim.x) {
+            float a[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) a[c] = blk_apply<NR_, NE_>(T + c * OSZ, sib + c * NR_, k);
+            Mall[(lev_off[l] + (long long)py * n + px) * NR_ + k] = (a[0] + a[1]) + (a[2] + a[3]);
+        }
+        if (threadIdx.x == 0) ctr[lev_off[l] + (long long)py * n + px] = 0u;  // ready for the next launch
+        bxl = px;
+        byl = py;
+    }
+}
+
+int up_level(int L) { return std::max(2, L - 2); }
+
+// dynamic shared memory of k_up at L levels (ntab M2M tables)
+size_t up_smem(int L, int NR, int NE, int ntab)
+{
+    const int cb = up_level(L), gs = 1 << (L - cb), G = gs * gs;
+    const size_t osz = (size_t)NE * NE + (size_t)(NR - NE) * (NR - NE);
+    int nm = 0;
+    for (int g = G; g >= 1; g /= 4) nm += g;
+    return ((size_t)NR * UP_WP + (size_t)ntab * 4 * osz + (size_t)G * UP_C + (size_t)std::max(nm, 4) * NR) *
+           sizeof(float);
+}
+
+
 __global__ void __launch_bounds__(128) k_top_l2l(float *__restrict__ Lfin, const float *__restrict__ Lpart,
                                                  const float *__restrict__ Tb, long long off2, long long off3,
                                                  long long part_stride, int nsplit, FmmDev f)
@@ -2634,166 +2813,19 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
 // indexed by depth (0 = leaf), the tables here by level of this grid.
 //
 // Three launches on the main stream beside the near field on the side
-// stream: k_fn_up (encoder and the whole upward pass), the resident M2L with
+// stream: k_up<24,16> (encoder and the whole upward pass), the resident M2L with
 // per-level tables, and k_fn_down (the whole downward pass, decoder, and the
 // join with the near field).
-constexpr int FN_UP_THREADS = 384;
 constexpr int FN_DOWN_THREADS = 256;
-constexpr int FN_WP = FN_C + 4;  // encoder row pitch in shared memory (floats)
 constexpr int FN_DN_CELLS = (FN_Z * 16 * 16 + FN_DOWN_THREADS - 1) / FN_DOWN_THREADS;  // cells per thread in k_fn_down
 
 namespace {
-
-// one output k of a block-diagonal map: sum_j T[blk][j][k] x[j] (T one
-// operator of [even NE x NE | odd NO x NO], input-major)
-// (T and x in shared memory)
-__device__ __forceinline__ float fn_apply(const float *T, const float *x, int k)
-{
-    if (k < FN_NE) {
-        float acc = 0.f;
-#pragma unroll
-        for (int j = 0; j < FN_NE; j++) acc = fmaf(T[j * FN_NE + k], x[j], acc);
-        return acc;
-    }
-    const int kk = k - FN_NE;
-    const float *To = T + FN_NE * FN_NE;
-    float acc = 0.f;
-#pragma unroll
-    for (int j = 0; j < FN_NO; j++) acc = fmaf(To[j * FN_NO + kk], x[FN_NE + j], acc);
-    return acc;
-}
 
 // stage n floats (n % 4 == 0, 16-byte aligned) into shared memory with
 // asynchronous copies; commit only (the caller waits)
 __device__ __forceinline__ void fn_stage(float *dst, const float *src, int n)
 {
     for (int i = threadIdx.x * 4; i < n; i += blockDim.x * 4) umma::cp_async16(umma::smem_u32(dst + i), src + i, true);
-}
-
-// Encoder and upward pass.  CTA = one box of level cb = max(2, L - 2), i.e.
-// gs x gs leaf boxes (gs = 2^(L - cb) <= 4): their charges and the encoder
-// weights are staged in shared memory, the leaf multipoles and every level
-// up to cb formed there and written out.  Levels above cb: the CTA that
-// completes the fourth child of a box forms that box (an arrival counter per
-// box; writers fence their stores before they arrive, the last arriver
-// fences before it reads the siblings through L2), and so on up to level 2.
-// No CTA waits for another.
-__global__ void __launch_bounds__(FN_UP_THREADS) k_fn_up(const float *__restrict__ rho, const float *__restrict__ W,
-                                                         const float *__restrict__ Tm2m, float *__restrict__ Mall,
-                                                         const long long *__restrict__ lev_off,
-                                                         unsigned *__restrict__ ctr, FmmDev f, int cb)
-{
-    extern __shared__ __align__(16) float fsm[];
-    const int gs = 1 << (f.L - cb), G = gs * gs, ncb = 1 << cb;
-    const int cbx = blockIdx.x % ncb, cby = blockIdx.x / ncb;  // the CTA's box at level cb
-    const int bx0 = cbx * gs, by0 = cby * gs;                  // its first leaf box
-    float *Ws = fsm;                       // [NR][FN_WP]: encoder rows, padded (conflict-free 16-byte reads)
-    float *Ts = Ws + FN_NR * FN_WP;        // M2M tables of parent levels 2 .. L-1: [L-2][4][OSZ]
-    float *q = Ts + (f.L - 2) * 4 * FN_OSZ;  // [G][C]
-    float *mb = q + G * FN_C;              // multipoles of levels L .. cb, G NR + G/4 NR + ...
-    __shared__ int s_last;
-    for (int i = threadIdx.x; i < FN_NR * FN_C / 4; i += blockDim.x) {
-        const int k = i / (FN_C / 4), c4 = i % (FN_C / 4);
-        umma::cp_async16(umma::smem_u32(Ws + k * FN_WP + 4 * c4), W + k * FN_C + 4 * c4, true);
-    }
-    fn_stage(Ts, Tm2m, (f.L - 2) * 4 * FN_OSZ);
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    pdl_begin();  // the weights above are constant; the charges are the predecessor's output
-    // charges, a region row at a time (consecutive threads on consecutive x);
-    // every load of a thread is issued before the first store
-    const int rw = gs * FN_S, ne = FN_Z * rw * rw;
-    constexpr int QR = (FN_Z * 32 * 32 + FN_UP_THREADS - 1) / FN_UP_THREADS;
-    float qv[QR];
-#pragma unroll
-    for (int r = 0; r < QR; r++) {
-        const int e = threadIdx.x + r * blockDim.x;
-        const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
-        const int x = bx0 * FN_S + rx, y = by0 * FN_S + ry;
-        qv[r] = (e < ne && x < f.X && y < f.Y) ? __ldg(&rho[((long long)lz * f.Y + y) * f.X + x]) : 0.f;
-    }
-#pragma unroll
-    for (int r = 0; r < QR; r++) {
-        const int e = threadIdx.x + r * blockDim.x;
-        if (e >= ne) break;
-        const int rx = e % rw, ry = (e / rw) % rw, lz = e / (rw * rw);
-        const int b = (ry / FN_S) * gs + rx / FN_S, c = lz * FN_S * FN_S + (ry % FN_S) * FN_S + rx % FN_S;
-        q[b * FN_C + c] = qv[r];
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
-    // encoder: four interleaved chains per output
-    const long long offL = lev_off[f.L];
-    for (int o = threadIdx.x; o < G * FN_NR; o += blockDim.x) {
-        const int b = o / FN_NR, k = o % FN_NR;
-        const float4 *qb = reinterpret_cast<const float4 *>(q + b * FN_C);
-        const float4 *wk = reinterpret_cast<const float4 *>(Ws + k * FN_WP);
-        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll 8
-        for (int c4 = 0; c4 < FN_C / 4; c4++) {
-            const float4 wv = wk[c4], qv4 = qb[c4];
-            a0 = fmaf(wv.x, qv4.x, a0);
-            a1 = fmaf(wv.y, qv4.y, a1);
-            a2 = fmaf(wv.z, qv4.z, a2);
-            a3 = fmaf(wv.w, qv4.w, a3);
-        }
-        const float v = (a0 + a1) + (a2 + a3);
-        mb[o] = v;
-        const int bx = bx0 + b % gs, by = by0 + b / gs;
-        Mall[(offL + (long long)by * f.nb + bx) * FN_NR + k] = v;
-    }
-    __syncthreads();
-    // levels L-1 .. cb inside the CTA
-    const float *child = mb;
-    float *par = mb + G * FN_NR;
-    int gc = gs;
-    for (int l = f.L - 1; l >= cb; l--) {
-        const int gp = gc / 2, n = 1 << l;
-        const float *T = Ts + (l - 2) * 4 * FN_OSZ;
-        const int px0 = bx0 >> (f.L - l), py0 = by0 >> (f.L - l);
-        for (int o = threadIdx.x; o < gp * gp * FN_NR; o += blockDim.x) {
-            const int p = o / FN_NR, k = o % FN_NR, px = p % gp, py = p / gp;
-            float v = 0.f;
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-                v += fn_apply(T + c * FN_OSZ, child + ((2 * py + (c >> 1)) * gc + 2 * px + (c & 1)) * FN_NR, k);
-            par[o] = v;
-            Mall[(lev_off[l] + (long long)(py0 + py) * n + px0 + px) * FN_NR + k] = v;
-        }
-        __syncthreads();
-        child = par;
-        par += gp * gp * FN_NR;
-        gc = gp;
-    }
-    // levels above cb: the last of four siblings to finish forms the parent
-    int bxl = cbx, byl = cby;
-    for (int l = cb - 1; l >= 2; l--) {
-        __threadfence();  // this CTA's multipoles are visible before it arrives
-        __syncthreads();
-        const int px = bxl >> 1, py = byl >> 1, n = 1 << l, nc = 2 * n;
-        if (threadIdx.x == 0) {
-            const unsigned t = atomicAdd(&ctr[lev_off[l] + (long long)py * n + px], 1u);
-            s_last = t == 3;
-        }
-        __syncthreads();
-        if (!s_last) return;
-        __threadfence();
-        float *sib = mb;  // the four children, read through L2
-        for (int i = threadIdx.x; i < 4 * FN_NR; i += blockDim.x) {
-            const int c = i / FN_NR, k = i % FN_NR;
-            sib[i] = __ldcg(&Mall[(lev_off[l + 1] + (long long)(2 * py + (c >> 1)) * nc + 2 * px + (c & 1)) * FN_NR + k]);
-        }
-        __syncthreads();
-        const float *T = Ts + (l - 2) * 4 * FN_OSZ;
-        for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) {
-            float v = 0.f;
-#pragma unroll
-            for (int c = 0; c < 4; c++) v += fn_apply(T + c * FN_OSZ, sib + c * FN_NR, k);
-            Mall[(lev_off[l] + (long long)py * n + px) * FN_NR + k] = v;
-        }
-        if (threadIdx.x == 0) ctr[lev_off[l] + (long long)py * n + px] = 0u;  // ready for the next launch
-        bxl = px;
-        byl = py;
-    }
 }
 
 // Downward pass, decoder and the join with the near field.  CTA = one box of
@@ -2892,7 +2924,7 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         __syncthreads();
         for (int l = 3; l <= L - 1; l++) {
             const float *T = Ts + (l - 3) * FN_OSZ;
-            for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) nxt[k] = Lc[(l - 2) * FN_NR + k] + fn_apply(T, cur, k);
+            for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) nxt[k] = Lc[(l - 2) * FN_NR + k] + blk_apply<FN_NR, FN_NE>(T, cur, k);
             __syncthreads();
             for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) cur[k] = nxt[k];
             __syncthreads();
@@ -2903,7 +2935,7 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         for (int i = threadIdx.x; i < 4 * FN_NR; i += blockDim.x) {
             const int c = i / FN_NR, k = i % FN_NR;
             const float *T = Ts + (L - 3 + c) * FN_OSZ;
-            leaf[c][k] = Lc[(L - 2 + c) * FN_NR + k] + fn_apply(T, cur, k);
+            leaf[c][k] = Lc[(L - 2 + c) * FN_NR + k] + blk_apply<FN_NR, FN_NE>(T, cur, k);
         }
     }
     __syncthreads();
@@ -2925,17 +2957,6 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         for (int k = 0; k < FN_NR; k++) acc = fmaf(Vs[k * FN_C + c], lb[k], acc);
         phi[cell] = acc;
     }
-}
-
-int fn_up_level(int L) { return std::max(2, L - 2); }
-
-size_t fn_up_smem(int L)
-{
-    const int cb = std::max(2, L - 2), gs = 1 << (L - cb), G = gs * gs;
-    int nm = 0;
-    for (int g = G; g >= 1; g /= 4) nm += g;
-    return ((size_t)FN_NR * FN_WP + (size_t)std::max(L - 2, 0) * 4 * FN_OSZ + (size_t)G * FN_C +
-            (size_t)std::max(nm, 4) * FN_NR) * sizeof(float);
 }
 
 size_t fn_down_smem(int L)
@@ -3020,9 +3041,9 @@ int farnet_bind(mms_ctx *ctx, const float *w, long long count)
         MMS_CUDA_TRY(cudaMemsetAsync(pl->fnLp, 0, nb * FN_NR * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->fnCtr, 0, nb * sizeof(unsigned), ctx->stream));
         MMS_TRY(m2l_res_prepare(FN_NR, FN_NE));
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_up, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)fn_up_smem(FN_DEPTHS + 1)));
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_up, cudaFuncAttributePreferredSharedMemoryCarveout,
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_up<FN_NR, FN_NE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)up_smem(FN_DEPTHS + 1, FN_NR, FN_NE, FN_DEPTHS - 1)));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_up<FN_NR, FN_NE>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                           cudaSharedmemCarveoutMaxShared));
         MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_down, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)fn_down_smem(FN_DEPTHS + 1)));
@@ -3059,10 +3080,11 @@ int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
         MMS_LAUNCH_CHECK(ctx);
         return MMS_OK;
     }
-    const int cb = fn_up_level(f.L);
-    MMS_CUDA_TRY(launch_k(k_fn_up, dim3(1u << (2 * cb)), dim3(FN_UP_THREADS), fn_up_smem(f.L), ctx->stream, rho,
-                          (const float *)pl->fnW, (const float *)pl->fnM2M, pl->fnM, (const long long *)pl->lev_dev,
-                          pl->fnCtr, f, cb));
+    const int cb = up_level(f.L);
+    MMS_CUDA_TRY(launch_k(k_up<FN_NR, FN_NE>, dim3(1u << (2 * cb)), dim3(UP_THREADS),
+                          up_smem(f.L, FN_NR, FN_NE, f.L - 2), ctx->stream, rho, (const float *)pl->fnW,
+                          (const float *)pl->fnM2M, 4LL * FN_OSZ, pl->fnM, (const long long *)pl->lev_dev, pl->fnCtr,
+                          f, cb));
     MMS_LAUNCH_CHECK(ctx);
     FmmDev fn = f;
     fn.NR = FN_NR;
