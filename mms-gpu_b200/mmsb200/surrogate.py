@@ -193,6 +193,16 @@ def evaluate(net, U, F, N2, P=None, batch=8):
     return dict(total_mean=float(np.mean(et)), total_max=float(np.max(et)))
 
 
+def lr_at(it, steps, lr_max, lr_min, warmup):
+    """step size of step `it` of `steps`: a linear warm-up over the first
+    `warmup` fraction (at least one step, never above lr_max), then a cosine
+    decay from lr_max to lr_min"""
+    w = it / max(1, steps - 1)
+    if w < warmup:
+        return lr_max * min(1.0, (it + 1) / max(1.0, warmup * steps))
+    return lr_min + 0.5 * (lr_max - lr_min) * (1 + math.cos(math.pi * (w - warmup) / (1 - warmup)))
+
+
 def train(U, F, N2, steps, batch=8, lr_max=1e-4, lr_min=1e-6, warmup=0.02, seed=1, weights=None, val=None,
           log_every=250, log=print):
     """fits the network (from `weights`, else the nested-SVD start) to the
@@ -232,11 +242,7 @@ def train(U, F, N2, steps, batch=8, lr_max=1e-4, lr_min=1e-6, warmup=0.02, seed=
         torch.index_select(U, 0, idx, out=ub)
         torch.index_select(F, 0, idx, out=fb)
         torch.index_select(N2, 0, idx, out=nb2)
-        w = it / max(1, steps - 1)
-        if w < warmup:
-            lr = lr_max * (it + 1) / (warmup * steps)
-        else:
-            lr = lr_min + 0.5 * (lr_max - lr_min) * (1 + math.cos(math.pi * (w - warmup) / (1 - warmup)))
+        lr = lr_at(it, steps, lr_max, lr_min, warmup)
         loss = net.train_step(ub, fb, nb2, batch, lr)
         if it % log_every == 0 or it == steps - 1:
             rec = dict(step=it, loss_rel=math.sqrt(max(loss, 0.0)), lr=lr, s=time.time() - t0)

@@ -75,3 +75,18 @@ def test_gradient_matches_finite_differences(oracle_mod, w0):
         for s in (16, 17, 18, 23, 24, 25, 30, 31, 32):
             o = off[("M2L", d)] + s * OF.OSZ
             assert not np.any(gr[o:o + OF.OSZ])
+
+
+def test_training_schedule_stays_within_lr_max():
+    """the warm-up + cosine schedule of the training driver: never above
+    lr_max, lr_max after the warm-up, lr_min at the last step, for long and
+    very short runs"""
+    from mmsb200.surrogate import lr_at
+    for steps in (1, 2, 3, 10, 4000):
+        lrs = [lr_at(i, steps, 1e-4, 1e-6, 0.02) for i in range(steps)]
+        assert max(lrs) <= 1e-4 * (1 + 1e-12), (steps, max(lrs))
+        assert min(lrs) >= 1e-6 * (1 - 1e-12)
+        if steps > 1:
+            assert abs(lrs[-1] - 1e-6) < 1e-12
+    lrs = [lr_at(i, 4000, 1e-4, 1e-6, 0.02) for i in range(4000)]
+    assert lrs[0] < 1e-6 * 2 and abs(max(lrs) - 1e-4) < 1e-9
