@@ -14,8 +14,9 @@
 // gradients are sums of outer products over boxes and samples, each family
 // one GEMM: the operands are gathered into K-major BF16 hi/lo planes
 // ([hi | lo | hi] against [hi | hi | lo], relative error ~2^-16 per product)
-// and multiplied by the tcgen05 core (umma_gemm_bf16); the block-diagonal
-// entries are then added into the gradient vector.
+// and multiplied by the tcgen05 core (umma_gemm_bf16_splitk: the long K
+// range, boxes x samples, split over CTAs, the partials summed in a fixed
+// order); the block-diagonal entries are then added into the gradient vector.
 #include <math.h>
 #include <string.h>
 
@@ -452,9 +453,8 @@ int forward(mms_farnet *n, const float *u, int nbatch)
     return MMS_OK;
 }
 
-int gemm_family(mms_farnet *n, const NetK &k, GatherP p, int fa, int fb, int d, const float *u)
+int gemm_family(mms_farnet *n, const NetK &k, GatherP p, int fa, int fb, int d)
 {
-    (void)u;
     p.Kp = (p.rows + 7) / 8 * 8;
     GatherP pa = p, pb = p;
     pa.side = 0;
@@ -510,20 +510,20 @@ int gradient(mms_farnet *n, const float *u, const float *far, const float *nrm2,
     p.l = n->L;
     p.rows = (long long)nbatch * nl;
     p.fam = FAM_W;
-    MMS_TRY(gemm_family(n, k, p, FN_C, FN_NR, 0, u));
+    MMS_TRY(gemm_family(n, k, p, FN_C, FN_NR, 0));
     p.fam = FAM_V;
-    MMS_TRY(gemm_family(n, k, p, FN_NR, FN_C, 0, u));
+    MMS_TRY(gemm_family(n, k, p, FN_NR, FN_C, 0));
     for (int l = 2; l <= n->L; l++) {
         p.l = l;
         p.n = 1 << l;
         p.rows = (long long)nbatch * p.n * p.n;
         p.fam = FAM_M2L;
-        MMS_TRY(gemm_family(n, k, p, 49 * FN_NR, FN_NR, n->L - l, u));
+        MMS_TRY(gemm_family(n, k, p, 49 * FN_NR, FN_NR, n->L - l));
         if (l < n->L) {
             p.fam = FAM_M2M;
-            MMS_TRY(gemm_family(n, k, p, 4 * FN_NR, FN_NR, n->L - l, u));
+            MMS_TRY(gemm_family(n, k, p, 4 * FN_NR, FN_NR, n->L - l));
             p.fam = FAM_L2L;
-            MMS_TRY(gemm_family(n, k, p, FN_NR, 4 * FN_NR, n->L - l, u));
+            MMS_TRY(gemm_family(n, k, p, FN_NR, 4 * FN_NR, n->L - l));
         }
     }
     std::vector<double> ls(nbatch), nh(nbatch);
