@@ -447,7 +447,8 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
     check), and the surrogate-assisted run the metric names (FMM check every
     50 steps, 1e-3 rel-L2 tolerance, FMM takes over above it), and the FMM at
     P = 5 and 6 (the orders whose error brackets the network's) with their
-    errors, each as K graph-replayed steps timed with CUDA events on the
+    errors, and the accurate network (24 + 16 channels) beside the FMM at
+    P = 8, each as K graph-replayed steps timed with CUDA events on the
     library's stream."""
     import torch
     import mmsb200
@@ -477,10 +478,10 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
             dctx.sync()
         out["demag_phi_rel_l2_vs_direct"] = float((phi_s.double() - phi_d.double()).norm() / phi_d.double().norm())
 
-    def steps_per_s(every, tol, nsteps, slv=solver):
+    def steps_per_s(every, tol, nsteps, slv=solver, weights=None):
         with mmsb200.Context(grid, params, slv, stream=stream.cuda_stream) as c:
             if every is not None:
-                c.set_surrogate(w, every, tol)
+                c.set_surrogate(w if weights is None else weights, every, tol)
             c.state_set(mask, M)
             c.run_fixed(args.dt, 3)
             c.sync()
@@ -509,10 +510,24 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
                                        "fallbacks": st["fallbacks"], "max_check_rel_l2_vs_fmm": st["max_err"],
                                        "surrogate_active_at_end": st["active"],
                                        "speedup_vs_fmm": v / fmm_value}
-    # the FMM at the orders that bracket the network's accuracy, on the same
-    # state and steps: what the network is worth at equal error
+    # the accurate network (24 + 16 channels, its nested-SVD start): error and
+    # steps/s on the same state and steps
+    wa, _ = S.load_weights(S.ACCURATE_WEIGHTS)
+    if wa is not None:
+        with mmsb200.Context(grid, params, solver, stream=stream.cuda_stream) as c:
+            c.set_surrogate(wa, 0, 1.0)
+            phi_a = torch.empty_like(rho)
+            c.potential_dev(rho, phi_a)
+            c.sync()
+            ea = float((phi_a.double() - phi_d.double()).norm() / phi_d.double().norm())
+        va, _ = steps_per_s(0, 1.0, n, weights=wa)
+        out["accurate_network"] = {"weights": os.path.basename(S.ACCURATE_WEIGHTS),
+                                   "channels": "24 even + 16 odd", "demag_phi_rel_l2_vs_direct": ea,
+                                   "steps_per_s": va}
+    # the FMM at the orders that bracket the networks' accuracy, on the same
+    # state and steps: what the networks are worth at equal error
     matched = []
-    for P in (5, 6):
+    for P in (5, 6, 8):
         slv = mmsb200.make_solver(mmsb200.SOLVER_FMM, P, 8)
         with mmsb200.Context(grid, params, slv, stream=stream.cuda_stream) as c:
             phi_f = torch.empty_like(rho)
@@ -520,8 +535,11 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
             c.sync()
             err = float((phi_f.double() - phi_d.double()).norm() / phi_d.double().norm())
         v, _ = steps_per_s(None, None, n, slv)
-        matched.append({"P": P, "leaf": 8, "demag_phi_rel_l2_vs_direct": err, "steps_per_s": v,
-                        "network_speedup": out["steps_per_s_surrogate_only"] / v})
+        row = {"P": P, "leaf": 8, "demag_phi_rel_l2_vs_direct": err, "steps_per_s": v,
+               "network_speedup": out["steps_per_s_surrogate_only"] / v}
+        if "accurate_network" in out:
+            row["accurate_network_speedup"] = out["accurate_network"]["steps_per_s"] / v
+        matched.append(row)
     out["fmm_at_matched_accuracy"] = matched
     return out
 

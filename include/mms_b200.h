@@ -325,8 +325,15 @@ int mms_farnet_train_step(mms_farnet *net, const float *u, const float *far, con
                           float lr, float beta1, float beta2, float eps, double *loss);
 long long mms_farnet_device_bytes(const mms_farnet *net);
 
-/* Binds trained weights to a context whose solver is MMS_SOLVER_SURROGATE
- * (leaf side 8, zdim 3, cubic cells) and arms its check: every `check_every`
+/* number of FP32 weights of the network of `width` channels the solver runs:
+ * 24 (16 even + 8 odd: the default, trained by mms_farnet_*) or 40 (24 + 16:
+ * the accurate one, 5-10x closer to the exact sum for a ~30 % longer
+ * evaluation); 0 for any other width */
+long long mms_surrogate_num_params(int width);
+
+/* Binds network weights to a context whose solver is MMS_SOLVER_SURROGATE
+ * (leaf side 8, zdim 3, cubic cells); `count` picks the width (see
+ * mms_surrogate_num_params).  It arms the network's check: every `check_every`
  * steps (0: never) of mms_run_fixed, and every `check_every` accepted steps
  * plus every rejected step of mms_march, the potential of the current state
  * is computed by both the network and the FMM (the solver's order P, leaf 8);

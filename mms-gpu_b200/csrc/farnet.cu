@@ -552,6 +552,13 @@ extern "C" {
 
 long long mms_farnet_num_params(void) { return fn_num_params(); }
 
+long long mms_surrogate_num_params(int width)
+{
+    if (width == FnTrain::NR) return FnTrain::num_params();
+    if (width == FnWide::NR) return FnWide::num_params();
+    return 0;
+}
+
 int mms_farnet_create(int xdim, int ydim, int batch, mms_farnet **out)
 {
     if (!out || xdim < 1 || ydim < 1 || batch < 1) {

@@ -13,16 +13,40 @@
 //                                  L2L [4][OSZ] (this depth's box -> child)
 // Depth 0 is the leaf level; a grid with L quadtree levels uses depth L - l
 // at level l.
+//
+// Two widths run in the solver (chosen by the length of the weight vector):
+//   24 = 16 even + 8 odd: the default, trained by the mms_farnet_* kernels;
+//   40 = 24 even + 16 odd: the accurate one, 5-10x closer to the exact sum
+//        for a ~30 % longer evaluation (its nested-SVD start, untrained).
+// FN_NE / FN_NO are the trainable (default) width.
 #pragma once
 
 constexpr int FN_S = 8, FN_Z = 3, FN_C = FN_S * FN_S * FN_Z;
 constexpr int FN_NE = 16, FN_NO = 8, FN_NR = FN_NE + FN_NO;
 constexpr int FN_OSZ = FN_NE * FN_NE + FN_NO * FN_NO;
 constexpr int FN_DEPTHS = 5;
+constexpr int FN_NR_MAX = 40;  // widest network the solver runs
 
-__host__ __device__ constexpr long long fn_off_W() { return 0; }
-__host__ __device__ constexpr long long fn_off_V() { return (long long)FN_C * FN_NR; }
-__host__ __device__ constexpr long long fn_off_M2L(int d) { return 2LL * FN_C * FN_NR + (long long)d * 49 * FN_OSZ; }
-__host__ __device__ constexpr long long fn_off_M2M(int d) { return fn_off_M2L(FN_DEPTHS) + (long long)(d - 1) * 8 * FN_OSZ; }
-__host__ __device__ constexpr long long fn_off_L2L(int d) { return fn_off_M2M(d) + 4LL * FN_OSZ; }
-__host__ __device__ constexpr long long fn_num_params() { return fn_off_M2M(FN_DEPTHS); }
+// weight layout of a network with NR_ channels, NE_ of them even
+template <int NR_, int NE_>
+struct FnShape {
+    static constexpr int NR = NR_, NE = NE_, NO = NR_ - NE_, OSZ = NE_ * NE_ + (NR_ - NE_) * (NR_ - NE_);
+    __host__ __device__ static constexpr long long off_W() { return 0; }
+    __host__ __device__ static constexpr long long off_V() { return (long long)FN_C * NR; }
+    __host__ __device__ static constexpr long long off_M2L(int d) { return 2LL * FN_C * NR + (long long)d * 49 * OSZ; }
+    __host__ __device__ static constexpr long long off_M2M(int d)
+    {
+        return off_M2L(FN_DEPTHS) + (long long)(d - 1) * 8 * OSZ;
+    }
+    __host__ __device__ static constexpr long long off_L2L(int d) { return off_M2M(d) + 4LL * OSZ; }
+    __host__ __device__ static constexpr long long num_params() { return off_M2M(FN_DEPTHS); }
+};
+using FnTrain = FnShape<FN_NR, FN_NE>;  // the trainable width
+using FnWide = FnShape<40, 24>;         // the accurate width
+
+__host__ __device__ constexpr long long fn_off_W() { return FnTrain::off_W(); }
+__host__ __device__ constexpr long long fn_off_V() { return FnTrain::off_V(); }
+__host__ __device__ constexpr long long fn_off_M2L(int d) { return FnTrain::off_M2L(d); }
+__host__ __device__ constexpr long long fn_off_M2M(int d) { return FnTrain::off_M2M(d); }
+__host__ __device__ constexpr long long fn_off_L2L(int d) { return FnTrain::off_L2L(d); }
+__host__ __device__ constexpr long long fn_num_params() { return FnTrain::num_params(); }

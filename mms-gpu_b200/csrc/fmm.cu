@@ -123,6 +123,7 @@ struct FmmPlan {
     float *fnM = nullptr;     // [boxes of all levels][NR] multipoles
     float *fnLp = nullptr;    // [boxes of all levels][NR] interaction-list locals
     unsigned *fnCtr = nullptr;  // [boxes] arrival counters of the upward pass (zero between launches)
+    int fn_nr = 0, fn_ne = 0;   // width of the bound network
     // algorithmic work per evaluation (for the roofline)
     double flops = 0;
     double stage_flops[5] = {0, 0, 0, 0, 0};  // P2M, M2M, M2L, L2L, L2P+P2P
@@ -1908,8 +1909,8 @@ int l2p_launch(const FmmDev &f, int nbx, int nby, const float *near, const float
     return MMS_ERR_ARG;
 }
 
-// resident-operator M2L specialisations: (NR, NE) for P = 1 .. 5
-#define MMS_M2L_RES_CASES(X) X(6, 4) X(12, 8) X(20, 12) X(24, 16) X(30, 18) X(42, 24)
+// resident-operator M2L specialisations: (NR, NE) for P = 1 .. 5 and the two network widths
+#define MMS_M2L_RES_CASES(X) X(6, 4) X(12, 8) X(20, 12) X(24, 16) X(30, 18) X(40, 24) X(42, 24)
 
 int m2l_res_supported(int NR, int NE)
 {
@@ -2834,6 +2835,7 @@ __device__ __forceinline__ void fn_stage(float *dst, const float *src, int n)
 // box's interaction-list local, one box per level), its leaves' locals, then
 // phi = near field (nnear partials, added in order) + V^T l_leaf at every
 // cell of the 16 x 16 x 3 region.
+template <int NR_, int NE_>
 __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__restrict__ Lp,
                                                              const float *__restrict__ Tl2l,
                                                              const float *__restrict__ V,
@@ -2841,7 +2843,8 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
                                                              long long near_stride, float *__restrict__ phi,
                                                              const long long *__restrict__ lev_off, FmmDev f)
 {
-    __shared__ float cur[FN_NR], nxt[FN_NR], leaf[4][FN_NR];
+    constexpr int OSZ_ = FnShape<NR_, NE_>::OSZ;
+    __shared__ float cur[NR_], nxt[NR_], leaf[4][NR_];
     extern __shared__ __align__(16) float dsm[];
     const int L = f.L;
     float *Vs = dsm;                  // [NR][C]
@@ -2849,19 +2852,19 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
     // ancestor's child position, then the 4 of level L-1 (the leaves'); they
     // and the decoder are constant, so they stream in while the predecessors
     // finish (group 0: tables, group 1: decoder)
-    float *Ts = Vs + FN_NR * FN_C;
-    float *Lc = Ts + (L > 2 ? (L + 1) * FN_OSZ : 0);  // interaction-list locals: ancestors 2..L-1, 4 leaves
+    float *Ts = Vs + NR_ * FN_C;
+    float *Lc = Ts + (L > 2 ? (L + 1) * OSZ_ : 0);  // interaction-list locals: ancestors 2..L-1, 4 leaves
     if (L > 2) {
         const int np = 1 << (L - 1), pbx = blockIdx.x % np, pby = blockIdx.x / np;
         for (int l = 3; l <= L - 1; l++) {
             const int sh = L - 1 - l, bx = pbx >> sh, by = pby >> sh;
             const int c = (by & 1) * 2 + (bx & 1);
-            fn_stage(Ts + (l - 3) * FN_OSZ, Tl2l + ((long long)(l - 1 - 2) * 4 + c) * FN_OSZ, FN_OSZ);
+            fn_stage(Ts + (l - 3) * OSZ_, Tl2l + ((long long)(l - 1 - 2) * 4 + c) * OSZ_, OSZ_);
         }
-        fn_stage(Ts + (L - 3) * FN_OSZ, Tl2l + (long long)(L - 1 - 2) * 4 * FN_OSZ, 4 * FN_OSZ);
+        fn_stage(Ts + (L - 3) * OSZ_, Tl2l + (long long)(L - 1 - 2) * 4 * OSZ_, 4 * OSZ_);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    fn_stage(Vs, V, FN_NR * FN_C);
+    fn_stage(Vs, V, NR_ * FN_C);
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     pdl_begin();
     // the near field of this CTA's cells, every load issued before anything waits
@@ -2892,8 +2895,8 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
     if (L > 2) {
         const int np = 1 << (L - 1), pbx = blockIdx.x % np, pby = blockIdx.x / np;
         // the CTA's chain, every load in flight at once: level l (2..L-1) ancestor, then the 4 leaves
-        for (int i = threadIdx.x; i < (L + 2) * (FN_NR / 4); i += blockDim.x) {
-            const int r = i / (FN_NR / 4), k4 = i % (FN_NR / 4);
+        for (int i = threadIdx.x; i < (L + 2) * (NR_ / 4); i += blockDim.x) {
+            const int r = i / (NR_ / 4), k4 = i % (NR_ / 4);
             long long box;
             if (r < L - 2) {
                 const int l = r + 2, sh = L - 1 - l;
@@ -2902,7 +2905,7 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
                 const int c = r - (L - 2);
                 box = lev_off[L] + (long long)(2 * pby + (c >> 1)) * (1 << L) + 2 * pbx + (c & 1);
             }
-            umma::cp_async16(umma::smem_u32(Lc + r * FN_NR + 4 * k4), Lp + box * FN_NR + 4 * k4, true);
+            umma::cp_async16(umma::smem_u32(Lc + r * NR_ + 4 * k4), Lp + box * NR_ + 4 * k4, true);
         }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");  // group 2: the chain
@@ -2915,27 +2918,27 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         lx0 = blockIdx.x % n;
         ly0 = blockIdx.x / n;
         nlf = 1;
-        for (int k = threadIdx.x; k < FN_NR; k += blockDim.x)
-            leaf[0][k] = Lp[(lev_off[L] + (long long)ly0 * n + lx0) * FN_NR + k];
+        for (int k = threadIdx.x; k < NR_; k += blockDim.x)
+            leaf[0][k] = Lp[(lev_off[L] + (long long)ly0 * n + lx0) * NR_ + k];
     } else {
         const int np = 1 << (L - 1);
         const int pbx = blockIdx.x % np, pby = blockIdx.x / np;
-        for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) cur[k] = Lc[k];
+        for (int k = threadIdx.x; k < NR_; k += blockDim.x) cur[k] = Lc[k];
         __syncthreads();
         for (int l = 3; l <= L - 1; l++) {
-            const float *T = Ts + (l - 3) * FN_OSZ;
-            for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) nxt[k] = Lc[(l - 2) * FN_NR + k] + blk_apply<FN_NR, FN_NE>(T, cur, k);
+            const float *T = Ts + (l - 3) * OSZ_;
+            for (int k = threadIdx.x; k < NR_; k += blockDim.x) nxt[k] = Lc[(l - 2) * NR_ + k] + blk_apply<NR_, NE_>(T, cur, k);
             __syncthreads();
-            for (int k = threadIdx.x; k < FN_NR; k += blockDim.x) cur[k] = nxt[k];
+            for (int k = threadIdx.x; k < NR_; k += blockDim.x) cur[k] = nxt[k];
             __syncthreads();
         }
         lx0 = 2 * pbx;
         ly0 = 2 * pby;
         nlf = 4;
-        for (int i = threadIdx.x; i < 4 * FN_NR; i += blockDim.x) {
-            const int c = i / FN_NR, k = i % FN_NR;
-            const float *T = Ts + (L - 3 + c) * FN_OSZ;
-            leaf[c][k] = Lc[(L - 2 + c) * FN_NR + k] + blk_apply<FN_NR, FN_NE>(T, cur, k);
+        for (int i = threadIdx.x; i < 4 * NR_; i += blockDim.x) {
+            const int c = i / NR_, k = i % NR_;
+            const float *T = Ts + (L - 3 + c) * OSZ_;
+            leaf[c][k] = Lc[(L - 2 + c) * NR_ + k] + blk_apply<NR_, NE_>(T, cur, k);
         }
     }
     __syncthreads();
@@ -2954,21 +2957,72 @@ __global__ void __launch_bounds__(FN_DOWN_THREADS) k_fn_down(const float *__rest
         float acc = nv[r];
         const float *lb = leaf[b];
 #pragma unroll 8
-        for (int k = 0; k < FN_NR; k++) acc = fmaf(Vs[k * FN_C + c], lb[k], acc);
+        for (int k = 0; k < NR_; k++) acc = fmaf(Vs[k * FN_C + c], lb[k], acc);
         phi[cell] = acc;
     }
 }
 
-size_t fn_down_smem(int L)
+size_t fn_down_smem(int L, int NR, int OSZ)
 {
-    return ((size_t)FN_NR * FN_C + (size_t)(L > 2 ? L + 1 : 0) * FN_OSZ + (size_t)(L + 2) * FN_NR) * sizeof(float);
+    return ((size_t)NR * FN_C + (size_t)(L > 2 ? L + 1 : 0) * OSZ + (size_t)(L + 2) * NR) * sizeof(float);
 }
+
+// the widths the solver runs: X(NR, NE)
+#define MMS_FN_WIDTHS(X) X(24, 16) X(40, 24)
 
 }  // namespace
 
-// Binds a weight vector (indexed by depth) to the context's plan: tables per
-// level of this grid, encoder scaled to physical units (phi = dx^2 net(rho)
-// for cubic cells), work buffers.  Leaf side 8 and 3 layers only.
+// tables per level of this grid from a weight vector of width Sh (encoder
+// scaled to physical units: phi = dx^2 net(rho) for cubic cells), into the
+// plan's buffers (sized for the widest network)
+template <class Sh>
+int farnet_tables(mms_ctx *ctx, const float *w)
+{
+    FmmPlan *pl = ctx->fmm;
+    const FmmDev &f = pl->d;
+    constexpr int NR = Sh::NR, OSZ = Sh::OSZ;
+    const int L = std::max(f.L, 2);
+    const int nlev = L - 1;  // levels 2..L
+    const double sc = ctx->g.dx * ctx->g.dx;
+    std::vector<float> W((size_t)FN_C * NR), V((size_t)NR * FN_C);
+    for (int c = 0; c < FN_C; c++)  // [c][k] -> [k][c]
+        for (int k = 0; k < NR; k++) W[(size_t)k * FN_C + c] = (float)(w[Sh::off_W() + c * NR + k] * sc);
+    for (size_t i = 0; i < V.size(); i++) V[i] = w[Sh::off_V() + i];
+    std::vector<float> M2L((size_t)nlev * 49 * OSZ), M2M((size_t)std::max(1, nlev - 1) * 4 * OSZ, 0.f),
+        L2L(M2M.size(), 0.f);
+    for (int l = 2; l <= L; l++) {
+        const int d = L - l;
+        memcpy(&M2L[(size_t)(l - 2) * 49 * OSZ], w + Sh::off_M2L(d), 49 * OSZ * sizeof(float));
+        if (l < L) {  // parent level l, depth d >= 1
+            memcpy(&M2M[(size_t)(l - 2) * 4 * OSZ], w + Sh::off_M2M(d), 4 * OSZ * sizeof(float));
+            memcpy(&L2L[(size_t)(l - 2) * 4 * OSZ], w + Sh::off_L2L(d), 4 * OSZ * sizeof(float));
+        }
+    }
+    // buffer sizes of the widest network, so that either width fits
+    constexpr int OSZ_MAX = FnWide::OSZ;
+    const size_t cap[5] = {(size_t)FN_C * FN_NR_MAX, (size_t)FN_NR_MAX * FN_C, (size_t)nlev * 49 * OSZ_MAX,
+                           (size_t)std::max(1, nlev - 1) * 4 * OSZ_MAX, (size_t)std::max(1, nlev - 1) * 4 * OSZ_MAX};
+    float **dst[5] = {&pl->fnW, &pl->fnV, &pl->fnM2L, &pl->fnM2M, &pl->fnL2L};
+    const std::vector<float> *src[5] = {&W, &V, &M2L, &M2M, &L2L};
+    for (int i = 0; i < 5; i++) {
+        if (!*dst[i]) {
+            if (cudaMalloc((void **)dst[i], cap[i] * sizeof(float)) != cudaSuccess) {
+                mms_set_error("surrogate: device allocation failed");
+                return MMS_ERR_NOMEM;
+            }
+            pl->bytes += cap[i] * sizeof(float);
+        }
+        MMS_CUDA_TRY(cudaMemcpyAsync(*dst[i], src[i]->data(), src[i]->size() * sizeof(float),
+                                     cudaMemcpyHostToDevice, ctx->stream));
+    }
+    pl->fn_nr = NR;
+    pl->fn_ne = Sh::NE;
+    return MMS_OK;
+}
+
+// Binds a weight vector (indexed by depth) to the context's plan.  Its length
+// picks the width: FnTrain (24 channels) or FnWide (32).  Leaf side 8 and 3
+// layers only.
 int farnet_bind(mms_ctx *ctx, const float *w, long long count)
 {
     FmmPlan *pl = ctx->fmm;
@@ -2986,72 +3040,70 @@ int farnet_bind(mms_ctx *ctx, const float *w, long long count)
         mms_set_error("surrogate: a grid of %d quadtree levels exceeds the network's %d depths", f.L, FN_DEPTHS);
         return MMS_ERR_ARG;
     }
-    const long long need = fn_num_params();
-    if (count != need) {
-        mms_set_error("surrogate: %lld weights given, the network has %lld", count, need);
+    if (count == FnTrain::num_params()) {
+        MMS_TRY(farnet_tables<FnTrain>(ctx, w));
+    } else if (count == FnWide::num_params()) {
+        MMS_TRY(farnet_tables<FnWide>(ctx, w));
+    } else {
+        mms_set_error("surrogate: %lld weights given; the networks have %lld (width %d) or %lld (width %d)", count,
+                      FnTrain::num_params(), FnTrain::NR, FnWide::num_params(), FnWide::NR);
         return MMS_ERR_ARG;
     }
-    if (!m2l_res_supported(FN_NR, FN_NE)) {
-        mms_set_error("surrogate: no resident M2L kernel for width %d", FN_NR);
-        return MMS_ERR_ARG;
-    }
-    const int L = std::max(f.L, 2);
-    const int nlev = L - 1;  // levels 2..L
-    const double sc = ctx->g.dx * ctx->g.dx;
-    std::vector<float> W((size_t)FN_C * FN_NR), V((size_t)FN_NR * FN_C);
-    for (int c = 0; c < FN_C; c++)  // [c][k] -> [k][c]
-        for (int k = 0; k < FN_NR; k++) W[(size_t)k * FN_C + c] = (float)(w[fn_off_W() + c * FN_NR + k] * sc);
-    for (size_t i = 0; i < V.size(); i++) V[i] = w[fn_off_V() + i];
-    std::vector<float> M2L((size_t)nlev * 49 * FN_OSZ), M2M((size_t)std::max(1, nlev - 1) * 4 * FN_OSZ, 0.f),
-        L2L(M2M.size(), 0.f);
-    for (int l = 2; l <= L; l++) {
-        const int d = L - l;
-        memcpy(&M2L[(size_t)(l - 2) * 49 * FN_OSZ], w + fn_off_M2L(d), 49 * FN_OSZ * sizeof(float));
-        if (l < L) {  // parent level l, depth d >= 1
-            memcpy(&M2M[(size_t)(l - 2) * 4 * FN_OSZ], w + fn_off_M2M(d), 4 * FN_OSZ * sizeof(float));
-            memcpy(&L2L[(size_t)(l - 2) * 4 * FN_OSZ], w + fn_off_L2L(d), 4 * FN_OSZ * sizeof(float));
-        }
-    }
-    auto up = [&](float **dst, const std::vector<float> &h) -> int {
-        if (!*dst) {
-            if (cudaMalloc((void **)dst, h.size() * sizeof(float)) != cudaSuccess) {
-                mms_set_error("surrogate: device allocation failed");
-                return MMS_ERR_NOMEM;
-            }
-            pl->bytes += h.size() * sizeof(float);
-        }
-        MMS_CUDA_TRY(cudaMemcpyAsync(*dst, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-        return MMS_OK;
-    };
-    MMS_TRY(up(&pl->fnW, W));
-    MMS_TRY(up(&pl->fnV, V));
-    MMS_TRY(up(&pl->fnM2L, M2L));
-    MMS_TRY(up(&pl->fnM2M, M2M));
-    MMS_TRY(up(&pl->fnL2L, L2L));
     if (!pl->fnM) {
         const size_t nb = (size_t)std::max(pl->nbox_total, 1LL);
-        if (cudaMalloc((void **)&pl->fnM, nb * FN_NR * sizeof(float)) != cudaSuccess ||
-            cudaMalloc((void **)&pl->fnLp, nb * FN_NR * sizeof(float)) != cudaSuccess ||
+        if (cudaMalloc((void **)&pl->fnM, nb * FN_NR_MAX * sizeof(float)) != cudaSuccess ||
+            cudaMalloc((void **)&pl->fnLp, nb * FN_NR_MAX * sizeof(float)) != cudaSuccess ||
             cudaMalloc((void **)&pl->fnCtr, nb * sizeof(unsigned)) != cudaSuccess) {
             mms_set_error("surrogate: device allocation failed");
             return MMS_ERR_NOMEM;
         }
-        pl->bytes += nb * (2 * FN_NR * sizeof(float) + sizeof(unsigned));
-        MMS_CUDA_TRY(cudaMemsetAsync(pl->fnM, 0, nb * FN_NR * sizeof(float), ctx->stream));
-        MMS_CUDA_TRY(cudaMemsetAsync(pl->fnLp, 0, nb * FN_NR * sizeof(float), ctx->stream));
+        pl->bytes += nb * (2 * FN_NR_MAX * sizeof(float) + sizeof(unsigned));
+        MMS_CUDA_TRY(cudaMemsetAsync(pl->fnM, 0, nb * FN_NR_MAX * sizeof(float), ctx->stream));
+        MMS_CUDA_TRY(cudaMemsetAsync(pl->fnLp, 0, nb * FN_NR_MAX * sizeof(float), ctx->stream));
         MMS_CUDA_TRY(cudaMemsetAsync(pl->fnCtr, 0, nb * sizeof(unsigned), ctx->stream));
-        MMS_TRY(m2l_res_prepare(FN_NR, FN_NE));
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_up<FN_NR, FN_NE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)up_smem(FN_DEPTHS + 1, FN_NR, FN_NE, FN_DEPTHS - 1)));
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_up<FN_NR, FN_NE>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                          cudaSharedmemCarveoutMaxShared));
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_down, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)fn_down_smem(FN_DEPTHS + 1)));
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_down, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                          cudaSharedmemCarveoutMaxShared));
+#define X(NR_, NE_)                                                                                              \
+    MMS_TRY(m2l_res_prepare(NR_, NE_));                                                                          \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_up<NR_, NE_>, cudaFuncAttributeMaxDynamicSharedMemorySize,              \
+                                      (int)up_smem(FN_DEPTHS + 1, NR_, NE_, FN_DEPTHS - 1)));                   \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_up<NR_, NE_>, cudaFuncAttributePreferredSharedMemoryCarveout,           \
+                                      cudaSharedmemCarveoutMaxShared));                                         \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_down<NR_, NE_>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                      (int)fn_down_smem(FN_DEPTHS + 1, NR_, FnShape<NR_, NE_>::OSZ)));         \
+    MMS_CUDA_TRY(cudaFuncSetAttribute(k_fn_down<NR_, NE_>, cudaFuncAttributePreferredSharedMemoryCarveout,      \
+                                      cudaSharedmemCarveoutMaxShared));
+        MMS_FN_WIDTHS(X)
+#undef X
     }
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     pl->fn_ready = 1;
+    return MMS_OK;
+}
+
+// the network's three launches at width Sh: upward pass, interaction lists,
+// downward pass + decoder + the join with the near field
+template <class Sh>
+int farnet_launch(mms_ctx *ctx, const float *rho, float *phi, const float *near, int nnear)
+{
+    FmmPlan *pl = ctx->fmm;
+    const FmmDev &f = pl->d;
+    constexpr int NR = Sh::NR, NE = Sh::NE, OSZ = Sh::OSZ;
+    const int cb = up_level(f.L);
+    MMS_CUDA_TRY(launch_k(k_up<NR, NE>, dim3(1u << (2 * cb)), dim3(UP_THREADS), up_smem(f.L, NR, NE, f.L - 2),
+                          ctx->stream, rho, (const float *)pl->fnW, (const float *)pl->fnM2M, 4LL * OSZ, pl->fnM,
+                          (const long long *)pl->lev_dev, pl->fnCtr, f, cb));
+    MMS_LAUNCH_CHECK(ctx);
+    FmmDev fn = f;
+    fn.NR = NR;
+    fn.NE = NE;
+    MMS_TRY(m2l_res_launch(fn, pl->n_res_items, pl->fnM, pl->fnLp, pl->fnM2L, pl->res_items, pl->lev_dev, ctx->stream,
+                           49LL * OSZ));
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
+    const unsigned ndown = f.L > 2 ? 1u << (2 * (f.L - 1)) : 1u << (2 * f.L);
+    MMS_CUDA_TRY(launch_k(k_fn_down<NR, NE>, dim3(ndown), dim3(FN_DOWN_THREADS), fn_down_smem(f.L, NR, OSZ),
+                          ctx->stream, (const float *)pl->fnLp, (const float *)pl->fnL2L, (const float *)pl->fnV, near,
+                          nnear, (long long)ctx->N, phi, (const long long *)pl->lev_dev, f));
+    MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
 
@@ -3080,26 +3132,8 @@ int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
         MMS_LAUNCH_CHECK(ctx);
         return MMS_OK;
     }
-    const int cb = up_level(f.L);
-    MMS_CUDA_TRY(launch_k(k_up<FN_NR, FN_NE>, dim3(1u << (2 * cb)), dim3(UP_THREADS),
-                          up_smem(f.L, FN_NR, FN_NE, f.L - 2), ctx->stream, rho, (const float *)pl->fnW,
-                          (const float *)pl->fnM2M, 4LL * FN_OSZ, pl->fnM, (const long long *)pl->lev_dev, pl->fnCtr,
-                          f, cb));
-    MMS_LAUNCH_CHECK(ctx);
-    FmmDev fn = f;
-    fn.NR = FN_NR;
-    fn.NE = FN_NE;
-    MMS_TRY(m2l_res_launch(fn, pl->n_res_items, pl->fnM, pl->fnLp, pl->fnM2L, pl->res_items, pl->lev_dev, ctx->stream,
-                           49LL * FN_OSZ));
-    MMS_LAUNCH_CHECK(ctx);
-    MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
-    const unsigned ndown = f.L > 2 ? 1u << (2 * (f.L - 1)) : 1u << (2 * f.L);
-    MMS_CUDA_TRY(launch_k(k_fn_down, dim3(ndown), dim3(FN_DOWN_THREADS), fn_down_smem(f.L), ctx->stream,
-                          (const float *)pl->fnLp,
-                          (const float *)pl->fnL2L, (const float *)pl->fnV, near, nnear, (long long)ctx->N, phi,
-                          (const long long *)pl->lev_dev, f));
-    MMS_LAUNCH_CHECK(ctx);
-    return MMS_OK;
+    if (pl->fn_nr == FnWide::NR) return farnet_launch<FnWide>(ctx, rho, phi, near, nnear);
+    return farnet_launch<FnTrain>(ctx, rho, phi, near, nnear);
 }
 
 int fmm_split_target(const mms_ctx *ctx, void **hi, void **lo, int *nbx, int *nby)

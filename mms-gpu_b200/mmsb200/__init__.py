@@ -123,6 +123,7 @@ SIGNATURES = {
     "mms_ens_autotune": (_I, [_VP, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_D)]),
     "mms_fmm_stage_times": (_I, [_VP, _VP, _VP, _I, ctypes.POINTER(_D)]),
     "mms_farnet_num_params": (ctypes.c_longlong, []),
+    "mms_surrogate_num_params": (ctypes.c_longlong, [_I]),
     "mms_farnet_create": (_I, [_I, _I, _I, ctypes.POINTER(_VP)]),
     "mms_farnet_destroy": (None, [_VP]),
     "mms_farnet_set_weights": (_I, [_VP, _VP, ctypes.c_longlong]),

@@ -44,30 +44,43 @@ import numpy as np
 S = 8                 # leaf side (cells)
 Z = 3                 # layers
 C = S * S * Z         # cells per leaf box, index c = z*64 + y*8 + x
-NE, NO = 16, 8        # even / odd channels
+NE, NO = 16, 8        # even / odd channels of the default (trainable) network
 NR = NE + NO
 OSZ = NE * NE + NO * NO
+WIDE = (24, 16)       # even / odd channels of the accurate network (its nested-SVD start)
 DEPTHS = 5            # depths 0..4: quadtrees of up to 6 levels (grids up to 512 cells a side)
 NSLOT = 49            # M2L offset slots (oy + 3) * 7 + (ox + 3); the 9 near ones stay zero
 
 
-def layout(depths=DEPTHS):
-    """offsets (in floats) of each table in the weight vector"""
+def layout(depths=DEPTHS, ne=None, no=None):
+    """offsets (in floats) of each table in the weight vector of a network
+    with ne even and no odd channels (default: NE, NO)"""
+    ne = NE if ne is None else ne
+    no = NO if no is None else no
+    nr, osz = ne + no, ne * ne + no * no
     off = {}
     o = 0
-    off["W"] = o; o += C * NR
-    off["V"] = o; o += NR * C
+    off["W"] = o; o += C * nr
+    off["V"] = o; o += nr * C
     for d in range(depths):
-        off[("M2L", d)] = o; o += NSLOT * OSZ
+        off[("M2L", d)] = o; o += NSLOT * osz
     for d in range(1, depths):
-        off[("M2M", d)] = o; o += 4 * OSZ
-        off[("L2L", d)] = o; o += 4 * OSZ
+        off[("M2M", d)] = o; o += 4 * osz
+        off[("L2L", d)] = o; o += 4 * osz
     off["total"] = o
     return off
 
 
-def num_params(depths=DEPTHS):
-    return layout(depths)["total"]
+def num_params(depths=DEPTHS, ne=None, no=None):
+    return layout(depths, ne, no)["total"]
+
+
+def width_of(count, depths=DEPTHS):
+    """(ne, no) of a weight vector of `count` floats: the default or the wide network"""
+    for ne, no in ((NE, NO), WIDE):
+        if num_params(depths, ne, no) == count:
+            return ne, no
+    raise ValueError(f"{count} weights match no network width")
 
 
 def slot(ox, oy):
@@ -108,11 +121,14 @@ def _leaf_kernels(cells, offsets):
     return out
 
 
-def h2_init(depths=DEPTHS, R=8, Rup=4):
-    """weight vector (float64) of the nested-SVD start"""
+def h2_init(depths=DEPTHS, R=8, Rup=4, ne=None, no=None):
+    """weight vector (float64) of the nested-SVD start with ne even and no odd
+    channels (default: NE, NO; WIDE for the accurate network)"""
+    ne = NE if ne is None else ne
+    no = NO if no is None else no
     cells = _cells()
     Pe, Po = _parity_frames()
-    width = (NE, NO)
+    width = (ne, no)
     # offsets each depth's compressed kernel is needed at: the M2L (|o| <= 3),
     # the next depth's basis (|2D + child| <= 2 Rup + 1) and its kernels
     need = {depths - 1: 3}
@@ -122,7 +138,7 @@ def h2_init(depths=DEPTHS, R=8, Rup=4):
     far = [(dx, dy) for dy in range(-R, R + 1) for dx in range(-R, R + 1) if max(abs(dx), abs(dy)) >= 2]
     Gf = _leaf_kernels(cells, far)
     U = []
-    for P, k in ((Pe, NE), (Po, NO)):
+    for P, k in ((Pe, ne), (Po, no)):
         A = np.concatenate([P.T @ g @ P for g in Gf], 1)
         U.append(P @ np.linalg.svd(A, full_matrices=False)[0][:, :k])
     del Gf
@@ -163,29 +179,30 @@ def h2_init(depths=DEPTHS, R=8, Rup=4):
                     Kd[(dx, dy)] = tuple(Ed[b].T @ coupled(Kc, (dx, dy), b) @ Ed[b] for b in (0, 1))
         Ks[d] = Kd
 
-    off = layout(depths)
+    off = layout(depths, ne, no)
+    osz = ne * ne + no * no
     w = np.zeros(off["total"])
     Ufull = np.concatenate(U, 1)  # C x NR, even channels first
-    w[off["W"]:off["W"] + C * NR] = Ufull.ravel()          # W[c][k]
-    w[off["V"]:off["V"] + NR * C] = Ufull.T.ravel()        # V[k][c]
+    w[off["W"]:off["W"] + C * (ne + no)] = Ufull.ravel()          # W[c][k]
+    w[off["V"]:off["V"] + (ne + no) * C] = Ufull.T.ravel()        # V[k][c]
     for d in range(depths):
-        t = np.zeros((NSLOT, OSZ))
+        t = np.zeros((NSLOT, osz))
         for oy in range(-3, 4):
             for ox in range(-3, 4):
                 if max(abs(ox), abs(oy)) < 2:
                     continue
                 Kd = Ks[d][(-ox, -oy)]  # source - target = -o; rows target channel, cols source channel
                 t[slot(ox, oy)] = pack_block(Kd[0].T, Kd[1].T)  # [j = source][k = target]
-        w[off[("M2L", d)]:off[("M2L", d)] + NSLOT * OSZ] = t.ravel()
+        w[off[("M2L", d)]:off[("M2L", d)] + NSLOT * osz] = t.ravel()
     for d in range(1, depths):
-        m2m = np.zeros((4, OSZ))
-        l2l = np.zeros((4, OSZ))
+        m2m = np.zeros((4, osz))
+        l2l = np.zeros((4, osz))
         for c in range(4):
             blocks = [E[d][b][c * width[b]:(c + 1) * width[b]] for b in (0, 1)]  # child channel x parent channel
             m2m[c] = pack_block(blocks[0], blocks[1])        # [j = child][k = parent]
             l2l[c] = pack_block(blocks[0].T, blocks[1].T)    # [j = parent][k = child]
-        w[off[("M2M", d)]:off[("M2M", d)] + 4 * OSZ] = m2m.ravel()
-        w[off[("L2L", d)]:off[("L2L", d)] + 4 * OSZ] = l2l.ravel()
+        w[off[("M2M", d)]:off[("M2M", d)] + 4 * osz] = m2m.ravel()
+        w[off[("L2L", d)]:off[("L2L", d)] + 4 * osz] = l2l.ravel()
     return w
 
 

@@ -29,7 +29,8 @@ MS = geometry.MS_PERMALLOY
 DX = 5e-9
 LEAF = 8
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "weights")
-DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "farnet_w24_d5.npz")
+DEFAULT_WEIGHTS = os.path.join(WEIGHTS_DIR, "farnet_w24_d5.npz")   # 16 + 8 channels: the default
+ACCURATE_WEIGHTS = os.path.join(WEIGHTS_DIR, "farnet_w40_d5.npz")  # 24 + 16 channels: 5-10x closer to exact
 
 
 # ---- training geometries ------------------------------------------------------
@@ -325,6 +326,11 @@ def main(argv=None):
     ap.add_argument("--time", action="store_true",
                     help="time one potential evaluation, network vs FMM, on the benchmark workload, and exit")
     ap.add_argument("--evals", type=int, default=50, help="evaluations timed with --time")
+    ap.add_argument("--weights", default="default",
+                    help="network timed with --time: default, accurate, or a weights file")
+    ap.add_argument("--start", choices=["default", "accurate"], default=None,
+                    help="write the nested-SVD start of that network (default: 16 + 8 channels, accurate: "
+                         "24 + 16) to --out, or to its shipped file, and exit")
     ap.add_argument("--pairs", type=int, default=4000)
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--batch", type=int, default=8)
@@ -333,8 +339,21 @@ def main(argv=None):
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--log", default=None)
     a = ap.parse_args(argv)
+    if a.start:
+        ne, no = (farnet.NE, farnet.NO) if a.start == "default" else farnet.WIDE
+        out = a.out if a.out != DEFAULT_WEIGHTS else (DEFAULT_WEIGHTS if a.start == "default" else ACCURATE_WEIGHTS)
+        save_weights(out, farnet.h2_init(ne=ne, no=no), dict(trained=0, width=ne + no, even=ne, odd=no,
+                                                             depths=farnet.DEPTHS))
+        print(json.dumps(dict(saved=out, weights=farnet.num_params(ne=ne, no=no))), flush=True)
+        return
     if a.time:
-        print(json.dumps(time_potential(a.evals)), flush=True)
+        path = {"default": DEFAULT_WEIGHTS, "accurate": ACCURATE_WEIGHTS}.get(a.weights, a.weights)
+        w, _ = load_weights(path)
+        if w is None:
+            raise SystemExit(f"no weights at {path}")
+        out = time_potential(a.evals, weights=w)
+        out["network"]["weights"] = os.path.basename(path)
+        print(json.dumps(out), flush=True)
         return
     logf = open(a.log, "w") if a.log else None
 

@@ -3,7 +3,8 @@ operator (the network of mms-gpu_b200/mmsb200/farnet.py and of the library's
 mms_farnet_* kernels): its forward pass, its relative-L2 loss and the gradient
 of that loss with respect to every weight, written out adjoint by adjoint, plus
 the exact near field it is paired with.  It checks the GPU forward, gradient
-and inference kernels.
+and inference kernels.  Either network width (the default 16 + 8 channels or
+the accurate 24 + 16) is read off the length of the weight vector.
 
 The far field it replaces is the reference's far-field pass (fmm_calc.cu:
 186-222, multipole-to-potential over the interaction lists of Box.cu:171-195);
@@ -18,64 +19,78 @@ import numpy as np
 
 S, Z = 8, 3
 C = S * S * Z
-NE, NO = 16, 8
+NE, NO = 16, 8          # the default network's even / odd channels
 NR = NE + NO
 OSZ = NE * NE + NO * NO
+WIDTHS = ((16, 8), (24, 16))  # the default and the accurate network
 NSLOT = 49
 CHILD = [(0, 0), (1, 0), (0, 1), (1, 1)]  # (cx, cy), index cy * 2 + cx
 
 
-def _layout(depths):
+def _layout(depths, ne=NE, no=NO):
+    nr, osz = ne + no, ne * ne + no * no
     off, o = {}, 0
-    off["W"] = o; o += C * NR
-    off["V"] = o; o += NR * C
+    off["W"] = o; o += C * nr
+    off["V"] = o; o += nr * C
     for d in range(depths):
-        off[("M2L", d)] = o; o += NSLOT * OSZ
+        off[("M2L", d)] = o; o += NSLOT * osz
     for d in range(1, depths):
-        off[("M2M", d)] = o; o += 4 * OSZ
-        off[("L2L", d)] = o; o += 4 * OSZ
+        off[("M2M", d)] = o; o += 4 * osz
+        off[("L2L", d)] = o; o += 4 * osz
     off["total"] = o
     return off
 
 
-def _full(v):
-    """one packed [even j][k] + [odd j][k] block pair -> full NR x NR [j][k]"""
-    T = np.zeros((NR, NR))
-    T[:NE, :NE] = v[:NE * NE].reshape(NE, NE)
-    T[NE:, NE:] = v[NE * NE:].reshape(NO, NO)
+def width_of(size, depths):
+    """(ne, no) of a weight vector of `size` floats"""
+    for ne, no in WIDTHS:
+        if _layout(depths, ne, no)["total"] == size:
+            return ne, no
+    raise AssertionError(f"{size} weights match no network width")
+
+
+def _full(v, ne, no):
+    """one packed [even j][k] + [odd j][k] block pair -> full (ne + no)^2 [j][k]"""
+    T = np.zeros((ne + no, ne + no))
+    T[:ne, :ne] = v[:ne * ne].reshape(ne, ne)
+    T[ne:, ne:] = v[ne * ne:].reshape(no, no)
     return T
 
 
-def _pack(T):
-    return np.concatenate([T[:NE, :NE].ravel(), T[NE:, NE:].ravel()])
+def _pack(T, ne):
+    return np.concatenate([T[:ne, :ne].ravel(), T[ne:, ne:].ravel()])
 
 
 def unpack(w, depths):
     w = np.asarray(w, np.float64)
-    off = _layout(depths)
-    assert w.size == off["total"], (w.size, off["total"])
-    t = {"W": w[off["W"]:off["W"] + C * NR].reshape(C, NR),
-         "V": w[off["V"]:off["V"] + NR * C].reshape(NR, C)}
+    ne, no = width_of(w.size, depths)
+    nr, osz = ne + no, ne * ne + no * no
+    off = _layout(depths, ne, no)
+    t = {"W": w[off["W"]:off["W"] + C * nr].reshape(C, nr),
+         "V": w[off["V"]:off["V"] + nr * C].reshape(nr, C), "ne": ne}
     for d in range(depths):
-        blk = w[off[("M2L", d)]:off[("M2L", d)] + NSLOT * OSZ].reshape(NSLOT, OSZ)
-        t[("M2L", d)] = np.stack([_full(b) for b in blk])
+        blk = w[off[("M2L", d)]:off[("M2L", d)] + NSLOT * osz].reshape(NSLOT, osz)
+        t[("M2L", d)] = np.stack([_full(b, ne, no) for b in blk])
     for d in range(1, depths):
         for name in ("M2M", "L2L"):
-            blk = w[off[(name, d)]:off[(name, d)] + 4 * OSZ].reshape(4, OSZ)
-            t[(name, d)] = np.stack([_full(b) for b in blk])
+            blk = w[off[(name, d)]:off[(name, d)] + 4 * osz].reshape(4, osz)
+            t[(name, d)] = np.stack([_full(b, ne, no) for b in blk])
     return t
 
 
 def pack(g, depths):
-    off = _layout(depths)
+    ne = g["ne"]
+    no = g["W"].shape[1] - ne
+    nr, osz = ne + no, ne * ne + no * no
+    off = _layout(depths, ne, no)
     w = np.zeros(off["total"])
-    w[off["W"]:off["W"] + C * NR] = g["W"].ravel()
-    w[off["V"]:off["V"] + NR * C] = g["V"].ravel()
+    w[off["W"]:off["W"] + C * nr] = g["W"].ravel()
+    w[off["V"]:off["V"] + nr * C] = g["V"].ravel()
     for d in range(depths):
-        w[off[("M2L", d)]:off[("M2L", d)] + NSLOT * OSZ] = np.concatenate([_pack(T) for T in g[("M2L", d)]])
+        w[off[("M2L", d)]:off[("M2L", d)] + NSLOT * osz] = np.concatenate([_pack(T, ne) for T in g[("M2L", d)]])
     for d in range(1, depths):
         for name in ("M2M", "L2L"):
-            w[off[(name, d)]:off[(name, d)] + 4 * OSZ] = np.concatenate([_pack(T) for T in g[(name, d)]])
+            w[off[(name, d)]:off[(name, d)] + 4 * osz] = np.concatenate([_pack(T, ne) for T in g[(name, d)]])
     return w
 
 
@@ -137,7 +152,7 @@ def forward(w, u, depths=5):
     for l in range(2, L + 1):
         n = 1 << l
         T = t[("M2L", L - l)]
-        acc = np.zeros((n, n, NR))
+        acc = np.zeros((n, n, t["W"].shape[1]))
         for ox, oy in _offsets():
             acc += _il_mask(n, ox, oy) * (_shift(M[l], ox, oy) @ T[(oy + 3) * 7 + ox + 3])
         Lp[l] = acc
@@ -164,7 +179,8 @@ def loss_and_gradient(w, batch, depths=5):
         _, Y, X = r.shape
         L, t, M, Lf, q = a["L"], a["t"], a["M"], a["Lf"], a["q"]
         dphi = boxes(2.0 * r / nrm2 / nb_, L)
-        gr = {k: np.zeros_like(v) for k, v in t.items()}
+        gr = {k: np.zeros_like(v) for k, v in t.items() if k != "ne"}
+        gr["ne"] = t["ne"]
         gr["V"] += np.einsum("abk,abc->kc", Lf[L], dphi)
         dLf = {L: dphi @ t["V"].T}
         for l in range(L, 2, -1):

@@ -14,6 +14,9 @@
   and more accurate than the plain FMM at its default (P = 4, leaf 8), which
   is what the network gains over the method without it; its potential
   evaluation is also faster than the FMM's.
+* The accurate network (24 + 16 channels, its own weights file): the same
+  pipeline against the oracle, within 2e-5 of the exact sum on held-out
+  states, 5x closer than the default, and faster than the FMM at P = 8.
 * Inside the time stepper: 10^4 surrogate-assisted steps of the benchmark
   workload (FMM check every 50 steps, tolerance 1e-3) with no fallback and
   the final magnetisation within 1 deg of the plain-FMM trajectory; an
@@ -35,6 +38,13 @@ def _weights():
     from mmsb200 import surrogate
     w, _ = surrogate.load_weights()
     assert w is not None, "network weights missing (mms-gpu_b200/weights)"
+    return w
+
+
+def _wide_weights():
+    from mmsb200 import surrogate
+    w, _ = surrogate.load_weights(surrogate.ACCURATE_WEIGHTS)
+    assert w is not None, "accurate network weights missing (mms-gpu_b200/weights)"
     return w
 
 
@@ -232,6 +242,78 @@ def test_trained_network_on_held_out_benchmark_states(cuda, lib):
     assert np.mean(e_sur) <= 1e-3 and np.max(e_sur) <= 1e-3
     assert np.mean(e_sur) < np.mean(e_fmm) and np.max(e_sur) < np.max(e_fmm)
     assert times["surrogate"] < times["fmm"], times
+
+
+@pytest.mark.parametrize("dims", [(70, 45), (256, 256)])
+def test_wide_network_potential_is_near_plus_network(cuda, lib, oracle_mod, dims):
+    """the accurate network (24 + 16 channels, picked by the weight count)
+    runs the same pipeline: phi = exact near field + dx^2 net(rho), against
+    the oracle's restatement of the same weights (3e-5: the tensor-core near
+    field's rounding)"""
+    import torch
+    import mmsb200
+    from mmsb200 import geometry
+    from oracle import farnet as OF
+    X, Y = dims
+    mask = geometry.random_blocks_mask(X, Y, 3, 0.3, 4, 5)
+    M = geometry.random_sphere(mask, 6)
+    w = _wide_weights()
+    rho = torch.zeros(3 * Y * X, device="cuda")
+    with _surrogate_ctx(mmsb200, mask, M, w, 0, 1.0) as ctx:
+        ctx.divergence_dev(torch.from_numpy(M.astype(np.float32)).cuda(), rho)
+        ps = torch.zeros_like(rho)
+        ctx.potential_dev(rho, ps)
+        ctx.sync()
+    r = rho.cpu().numpy().astype(np.float64).reshape(3, Y, X)
+    far, _ = OF.forward(w.astype(np.float64), r)
+    ref = DX * DX * (OF.near_field(r) + far)
+    assert rel_l2(ps.cpu().numpy().reshape(3, Y, X), ref) < 3e-5
+
+
+def test_wide_network_on_held_out_states_and_against_fmm_p8(cuda, lib):
+    """the accurate network on held-out states of the benchmark workload:
+    within 2e-5 of the exact sum (mean and max), at least 5x closer than the
+    default network, and its potential evaluation faster than the FMM's at
+    P = 8 (CUDA events, same stream), whose error it approaches"""
+    import torch
+    import mmsb200
+    states = held_out_states(5)
+    grid = mmsb200.Grid(256, 256, 3, DX, DX, DX)
+    e = {"wide": [], "default": [], "fmm8": []}
+    times = {}
+    with mmsb200.Context(grid, mmsb200.make_params(), mmsb200.make_solver(mmsb200.SOLVER_DIRECT)) as d, \
+            mmsb200.Context(grid, mmsb200.make_params(), mmsb200.make_solver(mmsb200.SOLVER_FMM, 8, 8)) as f8, \
+            mmsb200.Context(grid, mmsb200.make_params(), mmsb200.make_solver(mmsb200.SOLVER_SURROGATE, 6, 8)) as sw, \
+            mmsb200.Context(grid, mmsb200.make_params(), mmsb200.make_solver(mmsb200.SOLVER_SURROGATE, 6, 8)) as sd:
+        sw.set_surrogate(_wide_weights(), 0, 1.0)
+        sd.set_surrogate(_weights(), 0, 1.0)
+        for _, rho in states:
+            ex = torch.zeros_like(rho)
+            d.potential_dev(rho, ex)
+            for name, c in (("wide", sw), ("default", sd), ("fmm8", f8)):
+                p = torch.zeros_like(rho)
+                c.potential_dev(rho, p)
+                torch.cuda.synchronize()
+                e[name].append(float((p.double() - ex.double()).norm() / ex.double().norm()))
+        rho = states[-1][1]
+        out = torch.zeros_like(rho)
+        for name, c in (("wide", sw), ("fmm8", f8)):
+            stream = torch.cuda.current_stream()
+            for _ in range(5):
+                c.potential_dev(rho, out)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(50):
+                c.potential_dev(rho, out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times[name] = e0.elapsed_time(e1) / 50
+    print(f"accurate network: rel-L2 mean {np.mean(e['wide']):.3e} max {np.max(e['wide']):.3e}; default "
+          f"{np.mean(e['default']):.3e}; FMM P=8 {np.mean(e['fmm8']):.3e}; potential ms {times}")
+    assert np.max(e["wide"]) <= 2e-5
+    assert np.mean(e["wide"]) * 5 < np.mean(e["default"])
+    assert times["wide"] < times["fmm8"], times
 
 
 def test_assisted_run_1e4_steps_tracks_the_fmm(cuda, lib):

@@ -18,6 +18,12 @@ def w0():
     return farnet.h2_init()
 
 
+@pytest.fixture(scope="module")
+def w_wide():
+    from mmsb200 import farnet
+    return farnet.h2_init(ne=farnet.WIDE[0], no=farnet.WIDE[1])
+
+
 def _film(n, seed, oracle_mod, kind="lattice"):
     from mmsb200 import geometry
     if kind == "lattice":
@@ -35,6 +41,21 @@ def test_layout_matches_library(lib):
     from mmsb200 import farnet
     from oracle import farnet as OF
     assert farnet.num_params() == OF._layout(5)["total"] == mmsb200.FarNet.num_params()
+    L = mmsb200.load()
+    ne, no = farnet.WIDE
+    assert L.mms_surrogate_num_params(24) == farnet.num_params()
+    assert L.mms_surrogate_num_params(40) == farnet.num_params(ne=ne, no=no) == OF._layout(5, ne, no)["total"]
+    assert L.mms_surrogate_num_params(32) == 0
+    assert farnet.width_of(farnet.num_params(ne=ne, no=no)) == (ne, no)
+
+
+def test_shipped_weights_are_the_nested_svd_starts(w0, w_wide):
+    """the two weight files hold h2_init's starts (trained = 0 in their meta)"""
+    from mmsb200 import surrogate
+    for path, w in ((surrogate.DEFAULT_WEIGHTS, w0), (surrogate.ACCURATE_WEIGHTS, w_wide)):
+        got, meta = surrogate.load_weights(path)
+        assert got is not None and int(meta["trained"]) == 0
+        assert np.array_equal(got, w.astype(np.float32)), path
 
 
 @pytest.mark.parametrize("n,kind", [(64, "lattice"), (128, "lattice"), (64, "film")])
@@ -45,6 +66,20 @@ def test_nested_svd_start_is_accurate(oracle_mod, w0, n, kind):
     far, _ = OF.forward(w0, u)
     err = rel_l2(OF.near_field(u) + far, exact)
     assert err < (1e-4 if kind == "lattice" else 3e-4), err
+
+
+@pytest.mark.parametrize("n,kind", [(128, "lattice"), (64, "film")])
+def test_wide_start_is_ten_times_closer(oracle_mod, w0, w_wide, n, kind):
+    """the accurate network (24 + 16 channels): below 1e-5 on the disc
+    lattice, and at least 5x closer to the exact sum than the default"""
+    from oracle import farnet as OF
+    g, u = _film(n, 3, oracle_mod, kind)
+    exact = oracle_mod.potential_direct(g, u)
+    near = OF.near_field(u)
+    err = [rel_l2(near + OF.forward(w, u)[0], exact) for w in (w0, w_wide)]
+    if kind == "lattice":
+        assert err[1] < 1e-5, err
+    assert err[1] < err[0] / 5, err
 
 
 def test_gradient_matches_finite_differences(oracle_mod, w0):
