@@ -76,18 +76,52 @@ def workload(size, seed):
 
 # ---------------------------------------------------------------------------- clocks
 class ClockSampler:
-    """samples SM clocks and throttle reasons with nvidia-smi during the timed region"""
+    """samples SM clocks and throttle reasons during the timed region: NVML
+    read-only queries polled every millisecond on a background thread (a
+    timed region of a few milliseconds still gets samples), else nvidia-smi
+    every 200 ms"""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm MHz, reason bits)
+        self.smax = None
+        self.run = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = None
+            try:
+                import torch
+                bus = getattr(torch.cuda.get_device_properties(device_index), "pci_bus_id", None)
+                dom = getattr(torch.cuda.get_device_properties(device_index), "pci_domain_id", 0)
+                dev = getattr(torch.cuda.get_device_properties(device_index), "pci_device_id", 0)
+                if bus is not None:
+                    h = pynvml.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dev:02x}.0")
+            except Exception:
+                h = None
+            if h is None:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                         pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
+            self.nvml, self.h = pynvml, h
+        except Exception:
+            self.nvml = None
 
     def start(self):
+        if self.nvml is not None:
+            self.run = True
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -97,11 +131,29 @@ class ClockSampler:
         except (OSError, FileNotFoundError):
             self.proc = None
 
+    def _poll(self):
+        nv = self.nvml
+        while self.run:
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((sm, r))
+            except Exception:
+                pass
+            time.sleep(0.001)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.run = False
+            self.thread.join(timeout=5)
+            sm = [x for x, _ in self.samples]
+            reasons = {n for _, r in self.samples for n, bit in zip(self.NAMES, self.bits) if r & bit}
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.smax,
+                    "reasons": sorted(reasons), "samples": len(sm), "source": "nvml, 1 ms polling"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
@@ -111,7 +163,6 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for l in self.lines:
             p = [v.strip() for v in l.split(",")]
             if len(p) < 9:
@@ -121,11 +172,11 @@ class ClockSampler:
                 smax = float(p[2])
             except ValueError:
                 continue
-            for n, v in zip(names, p[5:9]):
+            for n, v in zip(self.NAMES, p[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ---------------------------------------------------------------------------- helpers
