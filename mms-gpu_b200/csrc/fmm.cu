@@ -1504,17 +1504,20 @@ __global__ void k_m2l_gather(const float *__restrict__ Mall, __nv_bfloat16 *__re
 // rows from T.  The three source box rows' partials go to separate buffers
 // that L2P adds in a fixed order.  Few CTAs (six per 128 boxes), so the
 // far-field chain that runs beside it keeps most SMs.
-constexpr int NTC_STAGES = 3;
+// pipeline stages: four (one more step in flight per SM) where 4 x (A + B
+// tiles) fits in shared memory, three at C = 256
+template <int BN>
+__host__ __device__ constexpr int ntc_stages() { return BN <= 192 ? 4 : 3; }
 
 // BN = C target cells of a box; a CTA takes half of them (N = BN / 2)
 template <int BN>
 struct NtcSmem {
-    alignas(1024) uint8_t ahi[NTC_STAGES][umma::BM * 128];
-    alignas(1024) uint8_t alo[NTC_STAGES][umma::BM * 128];
-    alignas(1024) uint8_t bhi[NTC_STAGES][(BN / 2) * 128];
-    alignas(1024) uint8_t blo[NTC_STAGES][(BN / 2) * 128];
-    uint64_t full[NTC_STAGES];  // the stage's four TMA copies landed
-    uint64_t done[NTC_STAGES];  // the MMAs reading the stage finished
+    alignas(1024) uint8_t ahi[ntc_stages<BN>()][umma::BM * 128];
+    alignas(1024) uint8_t alo[ntc_stages<BN>()][umma::BM * 128];
+    alignas(1024) uint8_t bhi[ntc_stages<BN>()][(BN / 2) * 128];
+    alignas(1024) uint8_t blo[ntc_stages<BN>()][(BN / 2) * 128];
+    uint64_t full[ntc_stages<BN>()];  // the stage's four TMA copies landed
+    uint64_t done[ntc_stages<BN>()];  // the MMAs reading the stage finished
     uint32_t tmem;
     int err;
     int last;                   // last step whose MMAs were committed (-1: none)
@@ -1593,7 +1596,7 @@ constexpr int NTC_TW = 32, NTC_TH = 4;  // CTA tile: 4 box rows x 32 boxes = the
 // layer-sz charges hi and lo, from the box-major copies, off-grid boxes read
 // as zero; the operator columns hi and lo of (dx, sz)) and issues R_hi T_hi
 // + R_lo T_hi + R_hi T_lo.  Its partial goes to [3 dy][N].  Thread 0 keeps
-// NTC_STAGES steps in flight and issues the MMAs.
+// ntc_stages<BN>() steps in flight and issues the MMAs.
 template <int BN>
 __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensorMap tm_hi,
                                                 const __grid_constant__ CUtensorMap tm_lo,
@@ -1605,6 +1608,7 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
     uint8_t *base = (uint8_t *)(((uintptr_t)raw_ntc + 1023) & ~(uintptr_t)1023);
     NtcSmem<BN> &s = *reinterpret_cast<NtcSmem<BN> *>(base);
     constexpr int C = BN, K3 = 3 * C, NH = BN / 2;     // NH target cells per CTA
+    constexpr int NS = ntc_stages<BN>();
     constexpr int TCOLS = NH <= 32 ? 32 : NH <= 64 ? 64 : NH <= 128 ? 128 : 256;  // allocation: a power of two
     constexpr uint32_t TX = 2 * (umma::BM + NH) * 128;  // bytes per step
     const int nk = 3 * f.Z;                             // steps: (dx, source layer)
@@ -1620,7 +1624,7 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
     if (tid == 0) {
-        for (int i = 0; i < NTC_STAGES; i++) {
+        for (int i = 0; i < NS; i++) {
             umma::mbar_init(&s.full[i]);
             umma::mbar_init(&s.done[i]);
         }
@@ -1635,7 +1639,7 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
     if (tid == 0) {
         const uint32_t idesc = umma::idesc_bf16(NH);
         auto issue = [&](int kt) {
-            const int st = kt % NTC_STAGES, dxi = kt / f.Z, sz = kt % f.Z, kc = dxi * C + sz * 64;
+            const int st = kt % NS, dxi = kt / f.Z, sz = kt % f.Z, kc = dxi * C + sz * 64;
             mbar_expect_tx(&s.full[st], TX);
             tma_load_4d(s.ahi[st], &tm_hi, 0, bx0 + dxi - 1, by0 + dyi - 1, sz, &s.full[st]);
             tma_load_4d(s.alo[st], &tm_lo, 0, bx0 + dxi - 1, by0 + dyi - 1, sz, &s.full[st]);
@@ -1644,10 +1648,10 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
         };
         bool ok = true;
         int issued = 0, landed = 0;
-        for (; issued < NTC_STAGES && issued < nk; issued++) issue(issued);
+        for (; issued < NS && issued < nk; issued++) issue(issued);
         for (int kt = 0; kt < nk && ok; kt++) {
-            const int st = kt % NTC_STAGES;
-            ok = umma::mbar_wait(&s.full[st], (uint32_t)((kt / NTC_STAGES) & 1));
+            const int st = kt % NS;
+            ok = umma::mbar_wait(&s.full[st], (uint32_t)((kt / NS) & 1));
             if (!ok) break;
             landed = kt + 1;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -1663,14 +1667,14 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
             umma::mma_commit(&s.done[st]);
             s.last = kt;
             // refill the stage of step kt - 1 once its MMAs are done (step kt's run meanwhile)
-            const int prev = kt - 1, nxt = prev + NTC_STAGES;
+            const int prev = kt - 1, nxt = prev + NS;
             if (prev >= 0 && nxt < nk) {
-                ok = umma::mbar_wait(&s.done[prev % NTC_STAGES], (uint32_t)((prev / NTC_STAGES) & 1));
+                ok = umma::mbar_wait(&s.done[prev % NS], (uint32_t)((prev / NS) & 1));
                 if (ok) issue(issued++);
             }
         }
         // after a timeout: let every copy still in flight land before the CTA's memory goes away
-        for (int kt = landed; kt < issued; kt++) umma::mbar_wait(&s.full[kt % NTC_STAGES], (uint32_t)((kt / NTC_STAGES) & 1));
+        for (int kt = landed; kt < issued; kt++) umma::mbar_wait(&s.full[kt % NS], (uint32_t)((kt / NS) & 1));
         if (!ok) s.err = 1;
     }
     __syncthreads();
@@ -1678,7 +1682,7 @@ __global__ void __launch_bounds__(128) k_p2p_tc(const __grid_constant__ CUtensor
     const int last = s.last;
     // the last commit covers every earlier MMA
     if (last >= 0) {
-        const bool fin = umma::mbar_wait(&s.done[last % NTC_STAGES], (uint32_t)((last / NTC_STAGES) & 1));
+        const bool fin = umma::mbar_wait(&s.done[last % NS], (uint32_t)((last / NS) & 1));
         ok = ok && fin;
     }
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
