@@ -147,7 +147,7 @@ def _surrogate_ctx(mmsb200, mask, M, w, every, tol, order=6, params=None):
     return ctx
 
 
-@pytest.mark.parametrize("dims", [(64, 64), (70, 45), (256, 256)])
+@pytest.mark.parametrize("dims", [(32, 32), (64, 64), (70, 45), (256, 256)])
 def test_solver_potential_is_near_plus_network(cuda, lib, oracle_mod, dims):
     """phi(surrogate) = exact near field + dx^2 net(rho) for cubic cells;
     within 3e-5: the near field runs on the tensor cores at leaf 8 (split-BF16
@@ -244,7 +244,7 @@ def test_trained_network_on_held_out_benchmark_states(cuda, lib):
     assert times["surrogate"] < times["fmm"], times
 
 
-@pytest.mark.parametrize("dims", [(70, 45), (256, 256)])
+@pytest.mark.parametrize("dims", [(32, 32), (70, 45), (256, 256)])
 def test_wide_network_potential_is_near_plus_network(cuda, lib, oracle_mod, dims):
     """the accurate network (24 + 16 channels, picked by the weight count)
     runs the same pipeline: phi = exact near field + dx^2 net(rho), against
