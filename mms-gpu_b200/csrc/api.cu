@@ -142,11 +142,13 @@ void drop_graph(mms_ctx *ctx)
     ctx->graph_kernels = 0;
 }
 
-// potential of the state M into ctx->phi
+// potential of the state M into ctx->phi (rho = div M into ctx->rho)
 int eval_state_potential(mms_ctx *ctx, const double *Mst)
 {
     MmsRange nvtx_("mms/field_evaluation");
     if (!ctx->p.demag) return MMS_OK;  // phi unused
+    if (ctx->s.kind == MMS_SOLVER_FMM || (ctx->s.kind == MMS_SOLVER_SURROGATE && !ctx->sur_active))
+        return launch_potential_fmm_state(ctx, Mst, ctx->rho, ctx->phi);
     MMS_TRY(launch_divergence_soa(ctx, Mst, ctx->rho));
     MMS_TRY(launch_potential(ctx, ctx->rho, ctx->phi));
     return MMS_OK;

@@ -95,7 +95,8 @@ __device__ __forceinline__ GridK inst_grid(const EnsInst &in, long long Ntot, do
 // (tile = blockIdx.x, blockIdx.x + gridDim.x, ...).
 __global__ void __launch_bounds__(ETPB) k_ens_div(const double *__restrict__ M, float *__restrict__ rho,
                                                   const EnsInst *__restrict__ inst, const EnsTile *__restrict__ tiles,
-                                                  int ntiles, long long Ntot, double dx, double dy, double dz)
+                                                  int ntiles, long long Ntot, double dx, double dy, double dz,
+                                                  DivScale h)
 {
   for (int tix = blockIdx.x; tix < ntiles; tix += gridDim.x) {
     const EnsTile tl = tiles[tix];
@@ -104,14 +105,8 @@ __global__ void __launch_bounds__(ETPB) k_ens_div(const double *__restrict__ M, 
     const long long i = tl.start + threadIdx.x;
     const long long plane = (long long)in.X * in.Y;
     const int x = (int)(i % in.X), y = (int)((i / in.X) % in.Y), z = (int)(i / plane);
-    const double *Mx = M + in.off, *My = M + Ntot + in.off, *Mz = M + 2 * Ntot + in.off;
-    const double x2 = (x != in.X - 1) ? Mx[i + 1] : 0.0;
-    const double x0 = (x != 0) ? Mx[i - 1] : 0.0;
-    const double y2 = (y != in.Y - 1) ? My[i + in.X] : 0.0;
-    const double y0 = (y != 0) ? My[i - in.X] : 0.0;
-    const double z2 = (z != in.Z - 1) ? Mz[i + plane] : 0.0;
-    const double z0 = (z != 0) ? Mz[i - plane] : 0.0;
-    rho[in.off + i] = (float)(0.5 * ((x2 - x0) / dx + (y2 - y0) / dy + (z2 - z0) / dz));
+    // the single-grid expression on the instance's planes
+    rho[in.off + i] = div_soa_cell(M + in.off, i, x, y, z, inst_grid(in, Ntot, dx, dy, dz), h);
   }
 }
 
@@ -492,7 +487,7 @@ int ens_potential(mms_ens *e, const double *Mst)
 {
     if (!e->p.demag) return MMS_OK;
     k_ens_div<<<e->grid_cells, ETPB, 0, e->stream>>>(Mst, e->rho, e->inst, e->tiles, e->ntiles, e->Ntot, e->dx, e->dy,
-                                                     e->dz);
+                                                     e->dz, div_scale(e->dx, e->dy, e->dz));
     ENS_LAUNCH_CHECK(e);
     return ens_direct(e);
 }
@@ -772,7 +767,7 @@ int mms_ens_autotune(mms_ens *e, int reps, int *ew, int *qrows, double *best_ms)
     }
     // the charges of the current state
     k_ens_div<<<e->grid_cells, ETPB, 0, e->stream>>>(e->M, e->rho, e->inst, e->tiles, e->ntiles, e->Ntot, e->dx, e->dy,
-                                                     e->dz);
+                                                     e->dz, div_scale(e->dx, e->dy, e->dz));
     ENS_LAUNCH_CHECK(e);
     cudaEvent_t e0, e1;
     MMS_CUDA_TRY(cudaEventCreate(&e0));

@@ -33,6 +33,7 @@
 #include "farnet.cuh"
 #include "fmm_ops.hpp"
 #include "mms_internal.cuh"
+#include "stencil_dev.cuh"
 #include "umma.cuh"
 
 namespace {
@@ -45,6 +46,38 @@ struct FmmDev {
     int X, Y;
     float inv_w;              // 1 / leaf width (m): L2P scale
 };
+
+// The divergence an upward-pass kernel forms from the FP64 state as it stages
+// the charges (the state path of a field evaluation, no separate divergence
+// launch): the state, its grid, and where rho and, when hi != nullptr, its
+// BF16 hi / lo split for the tensor-core near field go.
+struct DivSrc {
+    const double *M;
+    float *rho;
+    __nv_bfloat16 *hi, *lo;
+    GridK g;
+    mmsdev::DivScale h;
+    int nbx, nby;
+};
+
+// rho at cell (x, y, z) inside the grid (div_soa_cell: the bits of the
+// divergence kernel), and its stores
+__device__ __forceinline__ float div_value(const DivSrc &dv, int x, int y, int z)
+{
+    const long long i = ((long long)z * dv.g.Y + y) * dv.g.X + x;
+    return mmsdev::div_soa_cell(dv.M, i, x, y, z, dv.g, dv.h);
+}
+
+__device__ __forceinline__ void div_store(const DivSrc &dv, int x, int y, int z, float v)
+{
+    dv.rho[((long long)z * dv.g.Y + y) * dv.g.X + x] = v;
+    if (dv.hi) {
+        const long long j = mmsdev::ntc_index(x, y, z, dv.nbx, dv.nby);
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        dv.hi[j] = h;
+        dv.lo[j] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
 
 // one GEMM of the grouped tensor-core M2L (a parity class x a parity block)
 struct TcGroup {
@@ -269,10 +302,12 @@ __device__ __forceinline__ void m2m_reduce(float *__restrict__ Mall, const float
 // the arithmetic of p2m_item / m2m_item.
 // Shared memory: charges [rows][C][PB], W [C][NR] when wsm, then (up) the M2M
 // operators and the per-parent M2M scratch.
-template <int PB>
+// DIV: the charges are the divergence of the state dv.M, formed here and also
+// stored to dv.rho (and its split) for the near field; rho is not read.
+template <int PB, bool DIV>
 __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, const float *__restrict__ Wg,
                                                  float *__restrict__ Mall, long long off_leaf, FmmDev f, int wsm,
-                                                 int up, const float *__restrict__ Tm2m, long long off_par)
+                                                 int up, const float *__restrict__ Tm2m, long long off_par, DivSrc dv)
 {
     extern __shared__ __align__(16) float q[];
     const int rows = up ? 2 : 1;
@@ -297,7 +332,32 @@ __global__ void __launch_bounds__(512) k_p2m_row(const float *__restrict__ rho, 
     // are the predecessor's output
     pdl_begin();
     const int bx0 = blockIdx.x * PB, by0 = rows * blockIdx.y;
-    {
+    if constexpr (DIV) {
+        // element e = (row, xx) as below; each thread forms up to DR values
+        // (all their state loads in flight) before it stores any
+        constexpr int DR = 8;
+        const int RW = PB * s, ntot = rows * f.Z * s * RW;
+        for (int base = 0; base < ntot; base += DR * blockDim.x) {
+            float v[DR];
+#pragma unroll
+            for (int k = 0; k < DR; k++) {
+                const int e = base + threadIdx.x + k * blockDim.x, row = e / RW, xx = e - row * RW;
+                const int yy = row % s, z = (row / s) % f.Z, r = row / (s * f.Z);
+                const int x = bx0 * s + xx, y = (by0 + r) * s + yy;
+                v[k] = (e < ntot && x < f.X && y < f.Y) ? div_value(dv, x, y, z) : 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < DR; k++) {
+                const int e = base + threadIdx.x + k * blockDim.x, row = e / RW, xx = e - row * RW;
+                if (e >= ntot) break;
+                const int yy = row % s, z = (row / s) % f.Z, r = row / (s * f.Z);
+                const int x = bx0 * s + xx, y = (by0 + r) * s + yy;
+                const int b = xx / s, cx = xx - b * s;
+                q[r * CB + (z * s + yy) * s * PB + cx * PB + b] = v[k];
+                if (x < f.X && y < f.Y) div_store(dv, x, y, z, v[k]);
+            }
+        }
+    } else {
         const int RW = PB * s, nrow = rows * f.Z * s;
         const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
         for (int row = threadIdx.x >> 5; row < nrow; row += nw) {
@@ -1963,7 +2023,8 @@ int m2l_res_launch(const FmmDev &f, int nitems, const float *Mall, float *Lout, 
 int fmm_set_carveout()
 {
     const int c = cudaSharedmemCarveoutMaxShared;
-    const void *k[] = {(const void *)k_p2m_row<4>, (const void *)k_p2m_row<BB>, (const void *)k_m2m_c,
+    const void *k[] = {(const void *)k_p2m_row<4, false>, (const void *)k_p2m_row<BB, false>,
+                       (const void *)k_p2m_row<4, true>, (const void *)k_p2m_row<BB, true>, (const void *)k_m2m_c,
                        (const void *)k_top_m2m,    (const void *)k_top_l2l,     (const void *)k_l2l_c,
                        (const void *)k_m2l_split,  (const void *)k_m2l_gather,  (const void *)k_m2l_gemm};
     for (const void *fn : k) MMS_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, c));
@@ -2302,8 +2363,10 @@ int fmm_plan_create(mms_ctx *ctx)
         MMS_TRY(far_prepare(ctx, pl));
     {
         // P2M with W staged and the fused parent M2M: at most 160 KB
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<BB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<BB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        MMS_CUDA_TRY(cudaFuncSetAttribute(k_p2m_row<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     }
     {
         const size_t tsz = 4 * cstride;
@@ -2538,6 +2601,59 @@ static int near_launch(mms_ctx *ctx, const float *rho, cudaStream_t st)
     return MMS_ERR_ARG;
 }
 
+// P2M (with the level L-1 M2M when p2m_up) from rho, or, with dv, from the
+// divergence of dv->M that the kernel forms and stores as it goes
+static int p2m_launch(mms_ctx *ctx, const float *rho, const DivSrc *dv)
+{
+    FmmPlan *pl = ctx->fmm;
+    const FmmDev &f = pl->d;
+    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
+    const size_t tsz = 4 * ((size_t)f.NE * f.NE + (size_t)(f.NR - f.NE) * (f.NR - f.NE));
+    const int KT = ((f.NR + 31) / 32) * 32;
+    const long long leaf_off = pl->lev_off[f.L];
+    const int up = p2m_up(pl);
+    const int rows = up ? 2 : 1;
+    // item width: 4 boxes where the boxes are large (leaf side >= 8) or
+    // the expansions long (NR > 32), for twice the CTAs; else 8
+    const int PB = (f.s >= 8 || f.NR > 32) ? 4 : BB;
+    const size_t extra = up ? tsz + (PB / 2) * (4 * (size_t)f.NR + 4 * (size_t)KT) : 0;
+    // without the parent step, long expansions read W through L1 as they
+    // go instead of staging all of it first
+    const int wsm = (f.C * f.NR) % 4 == 0 &&
+                    ((size_t)f.C * (rows * PB + f.NR) + extra) * sizeof(float) <= 160 * 1024;
+    const size_t smem = ((size_t)f.C * (rows * PB + (wsm ? f.NR : 0)) + extra) * sizeof(float);
+    const dim3 grid(div_up(nbx, PB), up ? div_up(nby, 2) : nby),
+        block(up ? (PB / 2) * 4 * KT : std::min(512, ((PB * f.NR + 31) / 32) * 32));
+    const long long off_par = up ? pl->lev_off[f.L - 1] : 0LL;
+    const DivSrc d0 = dv ? *dv : DivSrc{};
+#define P2M_ARGS grid, block, smem, ctx->stream, rho, (const float *)pl->Wt, pl->Mall, leaf_off, f, wsm, up, \
+                 (const float *)pl->Tm2m, off_par, d0
+    if (PB == 4 && dv)
+        MMS_CUDA_TRY(launch_k(k_p2m_row<4, true>, P2M_ARGS));
+    else if (PB == 4)
+        MMS_CUDA_TRY(launch_k(k_p2m_row<4, false>, P2M_ARGS));
+    else if (dv)
+        MMS_CUDA_TRY(launch_k(k_p2m_row<BB, true>, P2M_ARGS));
+    else
+        MMS_CUDA_TRY(launch_k(k_p2m_row<BB, false>, P2M_ARGS));
+#undef P2M_ARGS
+    MMS_LAUNCH_CHECK(ctx);
+    return MMS_OK;
+}
+
+// the near field on the side stream, after the work queued on the main one so
+// far; ev_join marks its end
+static int near_fork(mms_ctx *ctx, const float *rho)
+{
+    FmmPlan *pl = ctx->fmm;
+    MMS_CUDA_TRY(cudaEventRecord(pl->ev_fork, ctx->stream));
+    MMS_CUDA_TRY(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
+    MMS_TRY(near_launch(ctx, rho, pl->side));
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
+    return MMS_OK;
+}
+
 // One stage of the FMM potential: 0 P2M, 1 M2M (all levels), 2 M2L (all
 // levels), 3 L2L (all levels, with the M2L partial sums), 4 L2P + P2P.  Every
 // stage only reads what earlier stages wrote, so re-running one stage on
@@ -2555,31 +2671,9 @@ static int launch_fmm_stage(mms_ctx *ctx, int stage, const float *rho, float *ph
     const int nsplit = pl->m2l_tc ? pl->tc_ksplit : (pl->m2l_resident ? 1 : NSPLIT);
     if (stage < 4 && !far) return MMS_OK;
     switch (stage) {
-    case 0: {
-        const long long leaf_off = pl->lev_off[f.L];
-        const int up = p2m_up(pl);
-        const int rows = up ? 2 : 1;
-        // item width: 4 boxes where the boxes are large (leaf side >= 8) or
-        // the expansions long (NR > 32), for twice the CTAs; else 8
-        const int PB = (f.s >= 8 || f.NR > 32) ? 4 : BB;
-        const size_t extra = up ? tsz + (PB / 2) * (4 * (size_t)f.NR + 4 * (size_t)KT) : 0;
-        // without the parent step, long expansions read W through L1 as they
-        // go instead of staging all of it first
-        const int wsm = (f.C * f.NR) % 4 == 0 &&
-                        ((size_t)f.C * (rows * PB + f.NR) + extra) * sizeof(float) <= 160 * 1024;
-        const size_t smem = ((size_t)f.C * (rows * PB + (wsm ? f.NR : 0)) + extra) * sizeof(float);
-        const dim3 grid(div_up(nbx, PB), up ? div_up(nby, 2) : nby),
-            block(up ? (PB / 2) * 4 * KT : std::min(512, ((PB * f.NR + 31) / 32) * 32));
-        if (PB == 4)
-            MMS_CUDA_TRY(launch_k(k_p2m_row<4>, grid, block, smem, ctx->stream, rho, (const float *)pl->Wt, pl->Mall,
-                                  leaf_off, f, wsm, up, (const float *)pl->Tm2m, up ? pl->lev_off[f.L - 1] : 0LL));
-        else
-            MMS_CUDA_TRY(launch_k(k_p2m_row<BB>, grid, block, smem, ctx->stream, rho, (const float *)pl->Wt,
-                                  pl->Mall, leaf_off, f, wsm, up, (const float *)pl->Tm2m,
-                                  up ? pl->lev_off[f.L - 1] : 0LL));
-        MMS_LAUNCH_CHECK(ctx);
+    case 0:
+        MMS_TRY(p2m_launch(ctx, rho, nullptr));
         break;
-    }
     case 1: {
         // level L-1 is formed inside P2M when p2m_up(); levels 3 and 2 in one
         // launch when top_two()
@@ -2749,6 +2843,47 @@ int far_launch(mms_ctx *ctx, const float *rho)
     return MMS_ERR_ARG;
 }
 
+// The potential of an RK4 stage's state.  With the resident M2L, k_p2m_row
+// forms rho = div M as it stages the charges and stores rho and its BF16
+// split; the near field, which reads the split, forks after it and runs
+// beside M2M and M2L.  That saves the divergence launch on the chain (P = 4
+// and 5 at leaf 8: 4 % and 10 % more RK4 steps/s at 256 x 256 x 3).  The
+// longer M2L kernels (split FP32 at P = 6: 8 % fewer steps/s; tensor cores at
+// P = 8: no change) lose more from sharing the SMs with the near field, so
+// those plans, like the ones without the row P2M (generic leaf kernel, one
+// level, the fused far field), run the divergence kernel first and fork the
+// near field before the P2M.
+int launch_potential_fmm_state(mms_ctx *ctx, const double *M, float *rho, float *phi)
+{
+    MmsRange nvtx_("mms/fmm_potential");
+    FmmPlan *pl = ctx->fmm;
+    if (!pl) {
+        mms_set_error("FMM plan missing");
+        return MMS_ERR_ARG;
+    }
+    const FmmDev &f = pl->d;
+    if (leaf_threads(f) == 0 || f.L < 2 || pl->far_fused || !pl->m2l_resident) {
+        MMS_TRY(launch_divergence_soa(ctx, M, rho));
+        return launch_potential_fmm(ctx, rho, phi);
+    }
+    DivSrc dv{};
+    dv.M = M;
+    dv.rho = rho;
+    dv.g = ctx->gk();
+    dv.h = mmsdev::div_scale(ctx->g.dx, ctx->g.dy, ctx->g.dz);
+    void *hi = nullptr, *lo = nullptr;
+    if (fmm_split_target(ctx, &hi, &lo, &dv.nbx, &dv.nby)) {
+        dv.hi = (__nv_bfloat16 *)hi;
+        dv.lo = (__nv_bfloat16 *)lo;
+    }
+    MMS_TRY(p2m_launch(ctx, rho, &dv));
+    pl->split_of = dv.hi ? rho : nullptr;
+    MMS_TRY(near_fork(ctx, rho));
+    for (int st = 1; st < 4; st++) MMS_TRY(launch_fmm_stage(ctx, st, rho, phi));
+    MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
+    return l2p_launch_far(ctx, rho, phi);
+}
+
 // 1 when a bounded wait gave up since the plan was made: a grid barrier of the
 // fused far-field kernel, or an mbarrier wait of the tensor-core near field or
 // M2L (their flags are per device and cleared when such a plan is made)
@@ -2785,12 +2920,7 @@ int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi)
         return MMS_OK;
     }
     // fork: the near field on the side stream, the far-field chain on the main one
-    const int nbx = std::min(f.nb, (f.X + f.s - 1) / f.s), nby = std::min(f.nb, (f.Y + f.s - 1) / f.s);
-    MMS_CUDA_TRY(cudaEventRecord(pl->ev_fork, ctx->stream));
-    MMS_CUDA_TRY(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
-    MMS_TRY(near_launch(ctx, rho, pl->side));
-    MMS_LAUNCH_CHECK(ctx);
-    MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
+    MMS_TRY(near_fork(ctx, rho));
     if (pl->far_fused)
         MMS_TRY(far_launch(ctx, rho));
     else
@@ -3086,7 +3216,7 @@ int farnet_bind(mms_ctx *ctx, const float *w, long long count)
 // the network's three launches at width Sh: upward pass, interaction lists,
 // downward pass + decoder + the join with the near field
 template <class Sh>
-int farnet_launch(mms_ctx *ctx, const float *rho, float *phi, const float *near, int nnear)
+int farnet_launch(mms_ctx *ctx, const float *rho, float *phi)
 {
     FmmPlan *pl = ctx->fmm;
     const FmmDev &f = pl->d;
@@ -3096,6 +3226,8 @@ int farnet_launch(mms_ctx *ctx, const float *rho, float *phi, const float *near,
                           ctx->stream, rho, (const float *)pl->fnW, (const float *)pl->fnM2M, 4LL * OSZ, pl->fnM,
                           (const long long *)pl->lev_dev, pl->fnCtr, f, cb));
     MMS_LAUNCH_CHECK(ctx);
+    const float *near = pl->p2p_tc ? pl->near3 : pl->near;
+    const int nnear = pl->p2p_tc ? 3 : 1;
     FmmDev fn = f;
     fn.NR = NR;
     fn.NE = NE;
@@ -3122,22 +3254,17 @@ int launch_potential_surrogate(mms_ctx *ctx, const float *rho, float *phi)
         return MMS_ERR_NOT_READY;
     }
     const FmmDev &f = pl->d;
-    MMS_CUDA_TRY(cudaEventRecord(pl->ev_fork, ctx->stream));
-    MMS_CUDA_TRY(cudaStreamWaitEvent(pl->side, pl->ev_fork, 0));
-    MMS_TRY(near_launch(ctx, rho, pl->side));
-    MMS_LAUNCH_CHECK(ctx);
-    MMS_CUDA_TRY(cudaEventRecord(pl->ev_join, pl->side));
-    const float *near = pl->p2p_tc ? pl->near3 : pl->near;
-    const int nnear = pl->p2p_tc ? 3 : 1;
+    MMS_TRY(near_fork(ctx, rho));
     if (f.L < 2) {
         // no far field: every box is in every other's near zone
         MMS_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, pl->ev_join, 0));
-        k_sum_parts<<<(unsigned)div_up(ctx->N, 256), 256, 0, ctx->stream>>>(near, nnear, ctx->N, phi);
+        k_sum_parts<<<(unsigned)div_up(ctx->N, 256), 256, 0, ctx->stream>>>(pl->p2p_tc ? pl->near3 : pl->near,
+                                                                            pl->p2p_tc ? 3 : 1, ctx->N, phi);
         MMS_LAUNCH_CHECK(ctx);
         return MMS_OK;
     }
-    if (pl->fn_nr == FnWide::NR) return farnet_launch<FnWide>(ctx, rho, phi, near, nnear);
-    return farnet_launch<FnTrain>(ctx, rho, phi, near, nnear);
+    if (pl->fn_nr == FnWide::NR) return farnet_launch<FnWide>(ctx, rho, phi);
+    return farnet_launch<FnTrain>(ctx, rho, phi);
 }
 
 int fmm_split_target(const mms_ctx *ctx, void **hi, void **lo, int *nbx, int *nby)

@@ -162,6 +162,10 @@ int farnet_bind(mms_ctx *ctx, const float *w, long long count);
 int rel_l2_dev(mms_ctx *ctx, const float *a, const float *b, long long n, double *out);
 void fmm_plan_destroy(mms_ctx *ctx);
 int launch_potential_fmm(mms_ctx *ctx, const float *rho, float *phi);
+// FMM potential of the FP64 state M into phi, and rho = div M into rho: where
+// the plan allows, the P2M forms rho itself (with the BF16 split of the
+// tensor-core near field) instead of a divergence launch before it
+int launch_potential_fmm_state(mms_ctx *ctx, const double *M, float *rho, float *phi);
 // the tensor-core near field's box-major BF16 hi / lo charges, for a
 // divergence kernel to write beside rho: returns 0 when the plan has no
 // tensor-core near field; fmm_split_written(ctx, rho) records that they hold

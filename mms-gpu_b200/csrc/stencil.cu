@@ -147,7 +147,7 @@ __global__ void k_hfield_aos(const float *__restrict__ M, const float *__restric
 // rho = div M; with rhi != NULL also the BF16 hi / lo split of rho in the
 // box-major layout of the tensor-core near field ([Z][nby][nbx][8][8], leaf
 // side 8; the padding cells beyond the grid stay zero from the plan)
-__global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho, GridK g,
+__global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho, GridK g, DivScale h,
                           __nv_bfloat16 *__restrict__ rhi, __nv_bfloat16 *__restrict__ rlo, int nbx, int nby)
 {
     pdl_begin();
@@ -155,18 +155,10 @@ __global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho,
     if (i >= g.N) return;
     int x, y, z;
     cell_xyz(i, g, x, y, z);
-    const double *Mx = M, *My = M + g.N, *Mz = M + 2 * g.N;
-    const long long sy = g.X, sz = (long long)g.X * g.Y;
-    double x2 = (x != g.X - 1) ? Mx[i + 1] : 0.0;
-    double x0 = (x != 0) ? Mx[i - 1] : 0.0;
-    double y2 = (y != g.Y - 1) ? My[i + sy] : 0.0;
-    double y0 = (y != 0) ? My[i - sy] : 0.0;
-    double z2 = (z != g.Z - 1) ? Mz[i + sz] : 0.0;
-    double z0 = (z != 0) ? Mz[i - sz] : 0.0;
-    const float v = (float)(0.5 * ((x2 - x0) / g.dx + (y2 - y0) / g.dy + (z2 - z0) / g.dz));
+    const float v = div_soa_cell(M, i, x, y, z, g, h);
     rho[i] = v;
     if (rhi) {
-        const long long j = (((long long)z * nby + (y >> 3)) * nbx + (x >> 3)) * 64 + (y & 7) * 8 + (x & 7);
+        const long long j = ntc_index(x, y, z, nbx, nby);
         const __nv_bfloat16 h = __float2bfloat16_rn(v);
         rhi[j] = h;
         rlo[j] = __float2bfloat16_rn(v - __bfloat162float(h));
@@ -405,7 +397,8 @@ int launch_divergence_soa(mms_ctx *ctx, const double *M, float *rho)
     int nbx = 0, nby = 0;
     const int split = fmm_split_target(ctx, &hi, &lo, &nbx, &nby);
     MMS_CUDA_TRY(launch_k(k_div_soa, dim3(div_up(ctx->N, TPB)), dim3(TPB), 0, ctx->stream, M, rho, ctx->gk(),
-                          (__nv_bfloat16 *)(split ? hi : nullptr), (__nv_bfloat16 *)(split ? lo : nullptr), nbx, nby));
+                          div_scale(ctx->g.dx, ctx->g.dy, ctx->g.dz), (__nv_bfloat16 *)(split ? hi : nullptr),
+                          (__nv_bfloat16 *)(split ? lo : nullptr), nbx, nby));
     MMS_LAUNCH_CHECK(ctx);
     fmm_split_written(ctx, split ? rho : nullptr);
     return MMS_OK;

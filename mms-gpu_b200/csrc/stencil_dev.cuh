@@ -43,6 +43,42 @@ __device__ __forceinline__ void hext_at(const PhysK &p, const double *__restrict
     H[2] = b2 / p.mu0;
 }
 
+// half reciprocal cell sizes 1 / (2 dx), 1 / (2 dy), 1 / (2 dz): the central
+// difference weights of div_soa_cell, formed once on the host
+struct DivScale {
+    double hx, hy, hz;
+};
+inline DivScale div_scale(double dx, double dy, double dz) { return DivScale{0.5 / dx, 0.5 / dy, 0.5 / dz}; }
+
+// rho = div M at cell i = (x, y, z) of the FP64 SoA state (planes N apart):
+// central differences, zero outside the grid (vector_functions.cpp:8-28, in
+// FP64), as products with the half reciprocal sizes (no divide on the device)
+// rounded one by one (no contraction).  Every kernel that forms rho from the
+// state uses this expression, so they agree bit for bit.
+__device__ __forceinline__ float div_soa_cell(const double *__restrict__ M, long long i, int x, int y, int z,
+                                              const GridK &g, const DivScale &h)
+{
+    const double *Mx = M, *My = M + g.N, *Mz = M + 2 * g.N;
+    const long long sy = g.X, sz = (long long)g.X * g.Y;
+    const double x2 = (x != g.X - 1) ? Mx[i + 1] : 0.0;
+    const double x0 = (x != 0) ? Mx[i - 1] : 0.0;
+    const double y2 = (y != g.Y - 1) ? My[i + sy] : 0.0;
+    const double y0 = (y != 0) ? My[i - sy] : 0.0;
+    const double z2 = (z != g.Z - 1) ? Mz[i + sz] : 0.0;
+    const double z0 = (z != 0) ? Mz[i - sz] : 0.0;
+    const double a = __dmul_rn(__dsub_rn(x2, x0), h.hx);
+    const double b = __dmul_rn(__dsub_rn(y2, y0), h.hy);
+    const double c = __dmul_rn(__dsub_rn(z2, z0), h.hz);
+    return (float)__dadd_rn(__dadd_rn(a, b), c);
+}
+
+// index of cell (x, y, z) in the box-major BF16 charge layout of the
+// tensor-core near field, [Z][nby][nbx][8][8] (leaf side 8)
+__device__ __forceinline__ long long ntc_index(int x, int y, int z, int nbx, int nby)
+{
+    return (((long long)z * nby + (y >> 3)) * nbx + (x >> 3)) * 64 + (y & 7) * 8 + (x & 7);
+}
+
 // effective field at cell i from phi (FP32) and the FP64 stage state
 __device__ __forceinline__ void field_soa(const float *__restrict__ phi, const double *__restrict__ M, long long i,
                                           int x, int y, int z, const GridK &g, const PhysK &p, const double he[3],
