@@ -240,7 +240,11 @@ def test_autotune_on_steps(cuda, lib, oracle_mod):
                                      (72, 40, 4, 4)])
 def test_fused_far_field_is_bitwise_the_staged_one(cuda, lib, X, Y, P, s):
     """one cooperative launch (P2M .. L2L) gives the same bits as one launch per
-    stage and level, and the fused plan runs inside the step graph"""
+    stage and level, and the fused plan runs inside the step graph.  In the
+    RK4 steps the staged plan's P2M forms rho = div M (and the near field's
+    BF16 split) itself where the M2L is resident, while the fused plan runs
+    the divergence kernel first: equal states after the steps also show that
+    both form the same rho and split, on ragged grids and both near fields."""
     import torch
     import mmsb200
     from mmsb200 import geometry
