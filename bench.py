@@ -397,43 +397,55 @@ def run_ours(args):
     roof["potential_ms_cold_l2"] = pot_ms
 
     # e2e through the public API with host buffers: H2D of the state, one step,
-    # D2H of the state, every step
+    # D2H of the state, every step.  The headline uses the reference's own
+    # state layout (N Vector3 of FP32, as rk4_step takes and returns it); the
+    # same loop with the FP64 state calls is reported beside it.
     e2e = None
     if not args.no_e2e:
-        host_M = torch.from_numpy(ctx.state_get()[0]).pin_memory()
+        M64 = ctx.state_get()[0]
         host_mat = torch.from_numpy(mask.astype(np.uint8)).pin_memory()
-        dev_M = torch.empty(host_M.shape, dtype=torch.float64, device="cuda")
         dev_mat = torch.empty(host_mat.shape, dtype=torch.uint8, device="cuda")
-        out_M = torch.empty_like(host_M).pin_memory()
-        t = 0.0
-        # one untimed round trip first: a state set from the host has no
-        # potential yet, so these steps run the evaluate-first step graph,
-        # captured here (4 field evaluations per step either way)
-        dev_M.copy_(host_M, non_blocking=True)
-        dev_mat.copy_(host_mat, non_blocking=True)
-        ctx.state_set_dev(dev_mat, dev_M, t)
-        ctx.run_fixed(args.dt, 1, use_graph=True)
-        ctx.sync()
-        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(args.steps)]
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            ev2[k][0].record(stream)
+
+        def e2e_run(dtype, set_dev, get_dev):
+            host_M = torch.from_numpy(M64.astype(dtype)).pin_memory()
+            dev_M = torch.empty(host_M.shape, dtype=host_M.dtype, device="cuda")
+            out_M = torch.empty_like(host_M).pin_memory()
+            t = 0.0
+            # one untimed round trip first: a state set from the host has no
+            # potential yet, so these steps run the evaluate-first step graph,
+            # captured here (4 field evaluations per step either way)
             dev_M.copy_(host_M, non_blocking=True)
             dev_mat.copy_(host_mat, non_blocking=True)
-            ctx.state_set_dev(dev_mat, dev_M, t)
+            set_dev(dev_mat, dev_M, t)
             ctx.run_fixed(args.dt, 1, use_graph=True)
-            ctx.state_get_dev(dev_M)
-            out_M.copy_(dev_M, non_blocking=True)
-            ev2[k][1].record(stream)
-            t += args.dt
-        torch.cuda.synchronize()
-        e2e_ms = max_over_ranks(ws, float(sum(a.elapsed_time(b) for a, b in ev2)))
-        e2e = {"value": ws * args.steps / (e2e_ms * 1e-3), "unit": "steps/s",
-               "h2d_bytes_per_step": int(host_M.numel() * 8 + host_mat.numel()),
-               "d2h_bytes_per_step": int(out_M.numel() * 8),
-               "path": "mms_state_set_dev + mms_run_fixed(1 step) + mms_state_get_dev, pinned host copies; "
-                       "4 field evaluations per step, as in the device-timed steps"}
+            ctx.sync()
+            ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(args.steps)]
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                ev2[k][0].record(stream)
+                dev_M.copy_(host_M, non_blocking=True)
+                dev_mat.copy_(host_mat, non_blocking=True)
+                set_dev(dev_mat, dev_M, t)
+                ctx.run_fixed(args.dt, 1, use_graph=True)
+                get_dev(dev_M)
+                out_M.copy_(dev_M, non_blocking=True)
+                ev2[k][1].record(stream)
+                t += args.dt
+            torch.cuda.synchronize()
+            ms = max_over_ranks(ws, float(sum(a.elapsed_time(b) for a, b in ev2)))
+            esz = host_M.element_size()
+            return {"value": ws * args.steps / (ms * 1e-3), "unit": "steps/s",
+                    "h2d_bytes_per_step": int(host_M.numel() * esz + host_mat.numel()),
+                    "d2h_bytes_per_step": int(out_M.numel() * esz)}
+
+        e2e = e2e_run(np.float32, ctx.state_set_f32_dev, ctx.state_get_f32_dev)
+        e2e["path"] = ("mms_state_set_f32_dev + mms_run_fixed(1 step) + mms_state_get_f32_dev, pinned host "
+                       "copies of M as N x 3 FP32 (the reference's Vector3 layout, as rk4_step takes it) and "
+                       "the material bytes; the state between the calls stays FP64 on the device; 4 field "
+                       "evaluations per step, as in the device-timed steps")
+        e2e["fp64_state_io"] = e2e_run(np.float64, ctx.state_set_dev, ctx.state_get_dev)
+        e2e["fp64_state_io"]["path"] = "the same with mms_state_set_dev / mms_state_get_dev (M as N x 3 FP64)"
 
     sur = None
     if args.solver == "fmm" and not args.no_surrogate:

@@ -149,6 +149,17 @@ int mms_state_get(mms_ctx *ctx, double *M, double *t);
 /* same with device pointers (material u8, M FP64 AoS) */
 int mms_state_set_dev(mms_ctx *ctx, const uint8_t *material, const double *M, double t);
 int mms_state_get_dev(mms_ctx *ctx, double *M);
+/* the state in the reference's own layout: M as N Vector3 of FP32
+ * (fptype = float, Vector3.h), the M and M2 arguments of rk4_step
+ * (ode_functions.cpp:76).  Set widens to the FP64 state exactly; get rounds
+ * each component to nearest.  The copies move half the bytes of the FP64
+ * calls; the state between steps stays FP64 on the device.  Host pointers,
+ * synchronous, like mms_state_set / mms_state_get: */
+int mms_state_set_f32(mms_ctx *ctx, const uint8_t *material, const float *M, double t);
+int mms_state_get_f32(mms_ctx *ctx, float *M, double *t);
+/* and with device pointers, asynchronous on the context's stream: */
+int mms_state_set_f32_dev(mms_ctx *ctx, const uint8_t *material, const float *M, double t);
+int mms_state_get_f32_dev(mms_ctx *ctx, float *M);
 /* nsteps classical RK4 steps of size dt, 4 field evaluations per step.  With
  * use_graph != 0 one step is captured once as a CUDA graph and replayed. */
 int mms_run_fixed(mms_ctx *ctx, double dt, int nsteps, int use_graph);

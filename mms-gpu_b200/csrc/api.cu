@@ -53,6 +53,29 @@ __global__ void k_soa_to_aos(const double *__restrict__ in, double *__restrict__
     out[3 * i + 2] = in[i + 2 * N];
 }
 
+// the reference's Vector3 layout: FP32 AoS (x,y,z per cell) -> FP64 SoA
+// planes, empty cells -> 0 (every float is exact in FP64)
+__global__ void k_aos32_to_soa(const float *__restrict__ in, const uint8_t *__restrict__ mat, double *__restrict__ out,
+                               long long N)
+{
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const bool m = mat[i] != 0;
+    out[i] = m ? (double)in[3 * i + 0] : 0.0;
+    out[i + N] = m ? (double)in[3 * i + 1] : 0.0;
+    out[i + 2 * N] = m ? (double)in[3 * i + 2] : 0.0;
+}
+
+// FP64 SoA planes -> FP32 AoS, each component rounded to nearest
+__global__ void k_soa_to_aos32(const double *__restrict__ in, float *__restrict__ out, long long N)
+{
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    out[3 * i + 0] = (float)in[i];
+    out[3 * i + 1] = (float)in[i + N];
+    out[3 * i + 2] = (float)in[i + 2 * N];
+}
+
 // per-block max over material cells of max_c |a_c - b_c|, then a fixed-order finish
 __global__ void k_maxdiff_part(const double *__restrict__ a, const double *__restrict__ b,
                                const uint8_t *__restrict__ mat, double *__restrict__ part, long long N)
@@ -650,6 +673,84 @@ int mms_state_get(mms_ctx *ctx, double *M, double *t)
         k_soa_to_aos<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->M, ctx->K, ctx->N);
         MMS_LAUNCH_CHECK(ctx);
         MMS_CUDA_TRY(cudaMemcpyAsync(M, ctx->K, 3 * (size_t)ctx->N * sizeof(double), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    }
+    double ts[TIME_SLOTS];
+    MMS_TRY(read_time(ctx, ts));
+    if (t) *t = ts[TIME_T];
+    double st[STAT_SLOTS];
+    MMS_TRY(read_stats(ctx, st));
+    if (st[7] != 0.0) {
+        mms_set_error("non-finite magnetisation produced by a step");
+        return MMS_ERR_NUMERIC;
+    }
+    return MMS_OK;
+}
+
+// ---- resident state in the reference's FP32 Vector3 layout ---------------------
+
+int mms_state_set_f32_dev(mms_ctx *ctx, const uint8_t *material, const float *M, double t)
+{
+    MmsRange nvtx_("mms/state_set_f32_dev");
+    if (!ctx || !material || !M) {
+        mms_set_error("NULL argument");
+        return MMS_ERR_ARG;
+    }
+    MMS_CUDA_TRY(cudaMemcpyAsync(ctx->mat, material, (size_t)ctx->N, cudaMemcpyDeviceToDevice, ctx->stream));
+    k_aos32_to_soa<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(M, ctx->mat, ctx->M, ctx->N);
+    MMS_LAUNCH_CHECK(ctx);
+    k_set_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate, t, t, 0.0);
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_TRY(clear_numeric_flag(ctx));
+    ctx->state_ready = true;
+    ctx->phi_valid = false;
+    return MMS_OK;
+}
+
+int mms_state_get_f32_dev(mms_ctx *ctx, float *M)
+{
+    MmsRange nvtx_("mms/state_get_f32_dev");
+    MMS_TRY(require_state(ctx));
+    if (!M) {
+        mms_set_error("NULL argument");
+        return MMS_ERR_ARG;
+    }
+    k_soa_to_aos32<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->M, M, ctx->N);
+    MMS_LAUNCH_CHECK(ctx);
+    return MMS_OK;
+}
+
+// host FP32 I/O stages through the slope buffer K (3 N doubles, free between
+// steps): the floats travel as floats, half the bytes of the FP64 path
+int mms_state_set_f32(mms_ctx *ctx, const uint8_t *material, const float *M, double t)
+{
+    if (!ctx || !material || !M) {
+        mms_set_error("NULL argument");
+        return MMS_ERR_ARG;
+    }
+    const size_t n = (size_t)ctx->N;
+    float *stage = reinterpret_cast<float *>(ctx->K);
+    MMS_CUDA_TRY(cudaMemcpyAsync(ctx->mat, material, n, cudaMemcpyHostToDevice, ctx->stream));
+    MMS_CUDA_TRY(cudaMemcpyAsync(stage, M, 3 * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    k_aos32_to_soa<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(stage, ctx->mat, ctx->M, ctx->N);
+    MMS_LAUNCH_CHECK(ctx);
+    k_set_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate, t, t, 0.0);
+    MMS_LAUNCH_CHECK(ctx);
+    MMS_TRY(clear_numeric_flag(ctx));
+    MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    ctx->state_ready = true;
+    ctx->phi_valid = false;
+    return MMS_OK;
+}
+
+int mms_state_get_f32(mms_ctx *ctx, float *M, double *t)
+{
+    MMS_TRY(require_state(ctx));
+    if (M) {
+        float *stage = reinterpret_cast<float *>(ctx->K);
+        k_soa_to_aos32<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->M, stage, ctx->N);
+        MMS_LAUNCH_CHECK(ctx);
+        MMS_CUDA_TRY(cudaMemcpyAsync(M, stage, 3 * (size_t)ctx->N * sizeof(float), cudaMemcpyDeviceToHost,
                                      ctx->stream));
     }
     double ts[TIME_SLOTS];

@@ -166,24 +166,14 @@ int rk4_step(const fptype t, const fptype dt, fptype *t2, const byte *material, 
     const mms_params p = ref_params(mu_0, Ms, Aexch, alfa, gamma, demag, exchange, external);
     mms_ctx *ctx = get_ctx(use_fmm, xdim, ydim, zdim, dx, dy, dz, P, p, verbosity);
     if (!ctx) return EXIT_FAILURE;
-    const size_t n = (size_t)xdim * ydim * zdim;
-    std::vector<double> m(3 * n);
-    for (size_t i = 0; i < n; i++) {
-        m[3 * i] = M[i].x;
-        m[3 * i + 1] = M[i].y;
-        m[3 * i + 2] = M[i].z;
-    }
     // k1 is evaluated from M at t, which is what the caller's H holds in every
-    // reference call site (ode_functions.cpp:230,267)
-    if (mms_state_set(ctx, material, m.data(), t) != MMS_OK) return fail("rk4_step");
-    if (mms_run_fixed(ctx, dt, 1, 0) != MMS_OK) return fail("rk4_step");
+    // reference call site (ode_functions.cpp:230,267).  M and M2 travel in the
+    // caller's FP32 Vector3 layout; the step runs on the FP64 state (one
+    // captured graph, replayed on every later call).
+    if (mms_state_set_f32(ctx, material, &M[0].x, t) != MMS_OK) return fail("rk4_step");
+    if (mms_run_fixed(ctx, dt, 1, 1) != MMS_OK) return fail("rk4_step");
     double tt = 0;
-    if (mms_state_get(ctx, m.data(), &tt) != MMS_OK) return fail("rk4_step");
-    for (size_t i = 0; i < n; i++) {
-        M2[i].x = (fptype)m[3 * i];
-        M2[i].y = (fptype)m[3 * i + 1];
-        M2[i].z = (fptype)m[3 * i + 2];
-    }
+    if (mms_state_get_f32(ctx, &M2[0].x, &tt) != MMS_OK) return fail("rk4_step");
     *t2 = t + dt;
     return EXIT_SUCCESS;
 }
@@ -194,18 +184,18 @@ struct MarchLog {
     mms_ctx *ctx;
     FILE *fh, *fhM, *fhp;
     int xdim, ydim, zdim;
-    std::vector<double> m;
+    std::vector<float> m;  // the state in the reference's FP32 Vector3 layout
     int status;
 };
 
 // helper_functions.cpp:107-123 layout: per z, x outer, y inner, "%g %g %g \n"
-void append_vector3d(FILE *fh, const double *m, int zdim, int ydim, int xdim)
+void append_vector3d(FILE *fh, const float *m, int zdim, int ydim, int xdim)
 {
     for (int z = 0; z < zdim; z++)
         for (int x = 0; x < xdim; x++)
             for (int y = 0; y < ydim; y++) {
                 const size_t i = (size_t)z * ydim * xdim + (size_t)y * xdim + x;
-                fprintf(fh, "%g %g %g \n", (fptype)m[3 * i], (fptype)m[3 * i + 1], (fptype)m[3 * i + 2]);
+                fprintf(fh, "%g %g %g \n", m[3 * i], m[3 * i + 1], m[3 * i + 2]);
             }
 }
 
@@ -220,7 +210,7 @@ int march_cb(void *user, int rejected, const mms_record *r)
         return 0;
     }
     double t;
-    if (mms_state_get(L->ctx, L->m.data(), &t) != MMS_OK) {
+    if (mms_state_get_f32(L->ctx, L->m.data(), &t) != MMS_OK) {
         L->status = EXIT_FAILURE;
         return 1;
     }
@@ -268,12 +258,7 @@ int time_marching(byte *material, Vector3 *M, const fptype finaltime, const fpty
     }
     const size_t n = (size_t)xdim * ydim * zdim;
     L.m.resize(3 * n);
-    for (size_t i = 0; i < n; i++) {
-        L.m[3 * i] = M[i].x;
-        L.m[3 * i + 1] = M[i].y;
-        L.m[3 * i + 2] = M[i].z;
-    }
-    int st = mms_state_set(ctx, material, L.m.data(), 0.0);
+    int st = mms_state_set_f32(ctx, material, &M[0].x, 0.0);
     if (st == MMS_OK) {
         mms_controller c;
         memset(&c, 0, sizeof c);
@@ -291,12 +276,7 @@ int time_marching(byte *material, Vector3 *M, const fptype finaltime, const fpty
     }
     if (st == MMS_OK) {
         double t;
-        st = mms_state_get(ctx, L.m.data(), &t);
-        for (size_t i = 0; i < n && st == MMS_OK; i++) {
-            M[i].x = (fptype)L.m[3 * i];
-            M[i].y = (fptype)L.m[3 * i + 1];
-            M[i].z = (fptype)L.m[3 * i + 2];
-        }
+        st = mms_state_get_f32(ctx, &M[0].x, &t);
     }
     fclose(L.fh);
     fclose(L.fhM);

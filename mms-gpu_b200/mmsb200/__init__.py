@@ -100,6 +100,10 @@ SIGNATURES = {
     "mms_state_get": (_I, [_VP, _VP, ctypes.POINTER(_D)]),
     "mms_state_set_dev": (_I, [_VP, _VP, _VP, _D]),
     "mms_state_get_dev": (_I, [_VP, _VP]),
+    "mms_state_set_f32": (_I, [_VP, _VP, _VP, _D]),
+    "mms_state_get_f32": (_I, [_VP, _VP, ctypes.POINTER(_D)]),
+    "mms_state_set_f32_dev": (_I, [_VP, _VP, _VP, _D]),
+    "mms_state_get_f32_dev": (_I, [_VP, _VP]),
     "mms_run_fixed": (_I, [_VP, _D, _I, _I]),
     "mms_state_stats": (_I, [_VP, ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D),
                              ctypes.POINTER(_D)]),
@@ -393,6 +397,25 @@ class Context:
 
     def state_get_dev(self, M):
         _check(load().mms_state_get_dev(self.h, _ptr(M)))
+
+    # the reference's FP32 Vector3 layout (N x 3 float32): half the bytes of
+    # the FP64 calls; the resident state stays FP64
+    def state_set_f32(self, material, M, t=0.0):
+        mat = np.ascontiguousarray(material, np.uint8)
+        M = np.ascontiguousarray(M, np.float32)
+        _check(load().mms_state_set_f32(self.h, _ptr(mat), _ptr(M), t))
+
+    def state_get_f32(self):
+        M = np.empty(self.grid.shape + (3,), np.float32)
+        t = ctypes.c_double()
+        _check(load().mms_state_get_f32(self.h, _ptr(M), ctypes.byref(t)))
+        return M, t.value
+
+    def state_set_f32_dev(self, material, M, t=0.0):
+        _check(load().mms_state_set_f32_dev(self.h, _ptr(material), _ptr(M), t))
+
+    def state_get_f32_dev(self, M):
+        _check(load().mms_state_get_f32_dev(self.h, _ptr(M)))
 
     def run_fixed(self, dt, nsteps, use_graph=True):
         _check(load().mms_run_fixed(self.h, dt, nsteps, int(use_graph)))

@@ -157,3 +157,37 @@ def test_numeric_error_is_reported(cuda, lib):
         with pytest.raises(mmsb200.MmsError) as e:
             ctx.state_get()
         assert e.value.status == mmsb200.MMS_ERR_NUMERIC
+
+
+def test_fp32_vector3_state_io(cuda, lib):
+    """the state in the reference's FP32 Vector3 layout (mms_state_*_f32,
+    host and device): set widens exactly, so the steps give the bits of the
+    FP64 calls; get rounds each component to nearest; empty cells read 0"""
+    import torch
+    import mmsb200
+    z = golden("rk4_16x16x3.npz")
+    dims, d = dims_of(z)
+    g = mmsb200.Grid(*dims, *d)
+    mat = z["material"]
+    M0 = np.asarray(z["M0"], np.float32).copy()
+    M0[mat == 0] = 1.0  # values at empty cells are dropped
+    dt = 1e-13
+    with mmsb200.Context(g, mmsb200.make_params(external=True)) as a, \
+            mmsb200.Context(g, mmsb200.make_params(external=True)) as b, \
+            mmsb200.Context(g, mmsb200.make_params(external=True)) as c:
+        a.state_set(mat, M0.astype(np.float64))
+        b.state_set_f32(mat, M0)
+        c.state_set_f32_dev(torch.from_numpy(mat.astype(np.uint8)).cuda(), torch.from_numpy(M0).cuda())
+        for ctx in (a, b, c):
+            ctx.run_fixed(dt, 3)
+        Ma, ta = a.state_get()
+        Mb, tb = b.state_get()
+        Mb32, tb32 = b.state_get_f32()
+        out = torch.empty(M0.shape, dtype=torch.float32, device="cuda")
+        c.state_get_f32_dev(out)
+        c.sync()
+        Mc32 = out.cpu().numpy()
+    assert np.array_equal(Ma, Mb) and ta == tb == tb32 and abs(ta - 3 * dt) < 1e-25
+    assert np.array_equal(Mb32, Ma.astype(np.float32))
+    assert np.array_equal(Mc32, Mb32)
+    assert np.all(Mb32[mat == 0] == 0) and np.all(Ma[mat == 0] == 0)
