@@ -367,6 +367,7 @@ struct mms_ens {
         k.external = p.external;
         k.n_hext = 0;
         k.ref_stage_time = 0;
+        physk_derive(k, dx, dy, dz);
         return k;
     }
 };

@@ -64,10 +64,28 @@ struct PhysK {
     double Ms, alpha, gamma, mu0;
     double cexch;        // 2 A / (mu0 Ms^2)
     double cdemag;       // 1 / (4 pi)
+    // the quotients of the per-cell field and LLG formed once on the host
+    // (physk_derive), so that the kernels multiply instead of divide
+    double hgx, hgy, hgz;  // cdemag / (2 d): the demag central difference
+    double ecx, ecy, ecz;  // cexch / d^2: the exchange Laplacian
+    double llg_a;          // alpha gamma / Ms
+    double inv_mu0;        // 1 / mu0: B -> H
     int demag, exchange, external;
     int n_hext;          // 0 + external: the reference's built-in ramp
     int ref_stage_time;
 };
+
+inline void physk_derive(PhysK &k, double dx, double dy, double dz)
+{
+    k.hgx = k.cdemag / (2 * dx);
+    k.hgy = k.cdemag / (2 * dy);
+    k.hgz = k.cdemag / (2 * dz);
+    k.ecx = k.cexch / (dx * dx);
+    k.ecy = k.cexch / (dy * dy);
+    k.ecz = k.cexch / (dz * dz);
+    k.llg_a = k.alpha * k.gamma / k.Ms;
+    k.inv_mu0 = 1.0 / k.mu0;
+}
 
 // time state kept on the device so a captured step graph stays valid:
 //   [0] t      current time of the state M

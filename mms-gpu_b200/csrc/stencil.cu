@@ -379,6 +379,7 @@ PhysK mms_ctx::pk() const
     k.external = p.external;
     k.n_hext = p.external ? (int)hext_t.size() : 0;
     k.ref_stage_time = p.ref_stage_time;
+    physk_derive(k, g.dx, g.dy, g.dz);
     return k;
 }
 

@@ -21,7 +21,7 @@ __device__ __forceinline__ void hext_at(const PhysK &p, const double *__restrict
     H[0] = H[1] = H[2] = 0.0;
     if (!p.external) return;
     if (p.n_hext == 0) {
-        H[0] = (1.0 / p.mu0) * ((t < 1e-9) ? (-0.3 / 1e-9 * t + 0.3) : 0.0);
+        H[0] = p.inv_mu0 * ((t < 1e-9) ? (-0.3 / 1e-9 * t + 0.3) : 0.0);
         return;
     }
     const int n = p.n_hext;
@@ -38,9 +38,9 @@ __device__ __forceinline__ void hext_at(const PhysK &p, const double *__restrict
         b1 = (1 - w) * tab[4 * k + 2] + w * tab[4 * (k + 1) + 2];
         b2 = (1 - w) * tab[4 * k + 3] + w * tab[4 * (k + 1) + 3];
     }
-    H[0] = b0 / p.mu0;
-    H[1] = b1 / p.mu0;
-    H[2] = b2 / p.mu0;
+    H[0] = b0 * p.inv_mu0;
+    H[1] = b1 * p.inv_mu0;
+    H[2] = b2 * p.inv_mu0;
 }
 
 // half reciprocal cell sizes 1 / (2 dx), 1 / (2 dy), 1 / (2 dz): the central
@@ -95,12 +95,11 @@ __device__ __forceinline__ void field_soa(const float *__restrict__ phi, const d
         double y0 = (y != 0) ? (double)phi[i - sy] : 0.0;
         double z2 = (z != g.Z - 1) ? (double)phi[i + sz] : 0.0;
         double z0 = (z != 0) ? (double)phi[i - sz] : 0.0;
-        H[0] += p.cdemag * (x2 - x0) / (2 * g.dx);
-        H[1] += p.cdemag * (y2 - y0) / (2 * g.dy);
-        H[2] += p.cdemag * (z2 - z0) / (2 * g.dz);
+        H[0] += p.hgx * (x2 - x0);
+        H[1] += p.hgy * (y2 - y0);
+        H[2] += p.hgz * (z2 - z0);
     }
     if (p.exchange) {
-        const double idx2 = 1.0 / (g.dx * g.dx), idy2 = 1.0 / (g.dy * g.dy), idz2 = 1.0 / (g.dz * g.dz);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const double *Mc = M + c * g.N;
@@ -111,7 +110,7 @@ __device__ __forceinline__ void field_soa(const float *__restrict__ phi, const d
             double ym = (y != 0) ? Mc[i - sy] : 0.0;
             double zp = (z != g.Z - 1) ? Mc[i + sz] : 0.0;
             double zm = (z != 0) ? Mc[i - sz] : 0.0;
-            H[c] += p.cexch * ((xp + xm - 2 * m0) * idx2 + (yp + ym - 2 * m0) * idy2 + (zp + zm - 2 * m0) * idz2);
+            H[c] += (xp + xm - 2 * m0) * p.ecx + (yp + ym - 2 * m0) * p.ecy + (zp + zm - 2 * m0) * p.ecz;
         }
     }
 }
@@ -125,7 +124,7 @@ __device__ __forceinline__ void llg(const double m[3], const double h[3], const 
     const double ex = m[1] * cz - m[2] * cy;
     const double ey = m[2] * cx - m[0] * cz;
     const double ez = m[0] * cy - m[1] * cx;
-    const double a = p.alpha * p.gamma / p.Ms;
+    const double a = p.llg_a;
     k[0] = -p.gamma * cx - a * ex;
     k[1] = -p.gamma * cy - a * ey;
     k[2] = -p.gamma * cz - a * ez;
