@@ -446,6 +446,15 @@ def run_ours(args):
                        "evaluations per step, as in the device-timed steps")
         e2e["fp64_state_io"] = e2e_run(np.float64, ctx.state_set_dev, ctx.state_get_dev)
         e2e["fp64_state_io"]["path"] = "the same with mms_state_set_dev / mms_state_get_dev (M as N x 3 FP64)"
+        # the bound the copies set: pinned H2D / D2H bandwidth of this box
+        # (32 MiB copies, best of 5, CUDA events) and the step time
+        h2d_gbs, d2h_gbs = pcie_bandwidth(stream)
+        bound = 1.0 / (ms_per_step * 1e-3 + e2e["h2d_bytes_per_step"] / (h2d_gbs * 1e9)
+                       + e2e["d2h_bytes_per_step"] / (d2h_gbs * 1e9))
+        e2e["pcie"] = {"h2d_gbs": h2d_gbs, "d2h_gbs": d2h_gbs, "bound_steps_per_s": bound,
+                       "frac_of_bound": e2e["value"] / bound,
+                       "note": "bound = 1 / (device step time + H2D bytes / H2D bandwidth + D2H bytes / D2H "
+                               "bandwidth): the copies and the step are serial in a round trip"}
 
     sur = None
     if args.solver == "fmm" and not args.no_surrogate:
@@ -605,6 +614,26 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
         matched.append(row)
     out["fmm_at_matched_accuracy"] = matched
     return out
+
+
+def pcie_bandwidth(stream, nbytes=32 << 20, reps=5):
+    """best pinned host <-> device copy bandwidth (GB/s) on this box, each way"""
+    import torch
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    out = []
+    for src, dst in ((h, d), (d, h)):
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            dst.copy_(src, non_blocking=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+        out.append(nbytes / (best * 1e-3) / 1e9)
+    return out[0], out[1]
 
 
 def bf16_peak():
