@@ -32,16 +32,29 @@ __global__ void k_set_time(double *tstate, double t, double tk1, double dt)
     tstate[TIME_DT] = dt;
 }
 
-// AoS (x,y,z per cell) FP64 -> SoA planes; empty cells -> 0
-__global__ void k_aos_to_soa(const double *__restrict__ in, const uint8_t *__restrict__ mat, double *__restrict__ out,
-                             long long N)
+// A new state in one launch: the material mask (mat_in -> mat, which may be
+// the same buffer), M from AoS (x,y,z per cell; FP64, or FP32 in the
+// reference's Vector3 layout, widened exactly) to the FP64 SoA planes with
+// empty cells -> 0, the time (t, t_k1 = t, dt = 0) and the non-finite flag
+// cleared
+template <typename T>
+__global__ void k_state_in(const T *__restrict__ in, const uint8_t *mat_in, uint8_t *mat, double *__restrict__ out,
+                           long long N, double *__restrict__ tstate, double *__restrict__ stats, double t)
 {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i == 0) {
+        tstate[TIME_T] = t;
+        tstate[TIME_TK1] = t;
+        tstate[TIME_DT] = 0.0;
+        stats[7] = 0.0;
+    }
     if (i >= N) return;
-    const bool m = mat[i] != 0;
-    out[i] = m ? in[3 * i + 0] : 0.0;
-    out[i + N] = m ? in[3 * i + 1] : 0.0;
-    out[i + 2 * N] = m ? in[3 * i + 2] : 0.0;
+    const uint8_t mv = mat_in[i];
+    mat[i] = mv;
+    const bool m = mv != 0;
+    out[i] = m ? (double)in[3 * i + 0] : 0.0;
+    out[i + N] = m ? (double)in[3 * i + 1] : 0.0;
+    out[i + 2 * N] = m ? (double)in[3 * i + 2] : 0.0;
 }
 
 __global__ void k_soa_to_aos(const double *__restrict__ in, double *__restrict__ out, long long N)
@@ -51,19 +64,6 @@ __global__ void k_soa_to_aos(const double *__restrict__ in, double *__restrict__
     out[3 * i + 0] = in[i];
     out[3 * i + 1] = in[i + N];
     out[3 * i + 2] = in[i + 2 * N];
-}
-
-// the reference's Vector3 layout: FP32 AoS (x,y,z per cell) -> FP64 SoA
-// planes, empty cells -> 0 (every float is exact in FP64)
-__global__ void k_aos32_to_soa(const float *__restrict__ in, const uint8_t *__restrict__ mat, double *__restrict__ out,
-                               long long N)
-{
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    const bool m = mat[i] != 0;
-    out[i] = m ? (double)in[3 * i + 0] : 0.0;
-    out[i + N] = m ? (double)in[3 * i + 1] : 0.0;
-    out[i + 2 * N] = m ? (double)in[3 * i + 2] : 0.0;
 }
 
 // FP64 SoA planes -> FP32 AoS, each component rounded to nearest
@@ -317,12 +317,6 @@ int require_state(mms_ctx *ctx)
         mms_set_error("state not set (call mms_state_set first)");
         return MMS_ERR_NOT_READY;
     }
-    return MMS_OK;
-}
-
-int clear_numeric_flag(mms_ctx *ctx)
-{
-    MMS_CUDA_TRY(cudaMemsetAsync(ctx->stats + 7, 0, sizeof(double), ctx->stream));
     return MMS_OK;
 }
 
@@ -621,13 +615,9 @@ int mms_state_set_dev(mms_ctx *ctx, const uint8_t *material, const double *M, do
         mms_set_error("NULL argument");
         return MMS_ERR_ARG;
     }
-    const size_t n = (size_t)ctx->N;
-    MMS_CUDA_TRY(cudaMemcpyAsync(ctx->mat, material, n, cudaMemcpyDeviceToDevice, ctx->stream));
-    k_aos_to_soa<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(M, ctx->mat, ctx->M, ctx->N);
+    k_state_in<double><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(M, material, ctx->mat, ctx->M, ctx->N,
+                                                                     ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
-    k_set_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate, t, t, 0.0);
-    MMS_LAUNCH_CHECK(ctx);
-    MMS_TRY(clear_numeric_flag(ctx));
     ctx->state_ready = true;
     ctx->phi_valid = false;
     return MMS_OK;
@@ -642,11 +632,9 @@ int mms_state_set(mms_ctx *ctx, const uint8_t *material, const double *M, double
     const size_t n = (size_t)ctx->N;
     MMS_CUDA_TRY(cudaMemcpyAsync(ctx->mat, material, n, cudaMemcpyHostToDevice, ctx->stream));
     MMS_CUDA_TRY(cudaMemcpyAsync(ctx->K, M, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    k_aos_to_soa<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->K, ctx->mat, ctx->M, ctx->N);
+    k_state_in<double><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->K, ctx->mat, ctx->mat, ctx->M, ctx->N,
+                                                                     ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
-    k_set_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate, t, t, 0.0);
-    MMS_LAUNCH_CHECK(ctx);
-    MMS_TRY(clear_numeric_flag(ctx));
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     ctx->state_ready = true;
     ctx->phi_valid = false;
@@ -696,12 +684,9 @@ int mms_state_set_f32_dev(mms_ctx *ctx, const uint8_t *material, const float *M,
         mms_set_error("NULL argument");
         return MMS_ERR_ARG;
     }
-    MMS_CUDA_TRY(cudaMemcpyAsync(ctx->mat, material, (size_t)ctx->N, cudaMemcpyDeviceToDevice, ctx->stream));
-    k_aos32_to_soa<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(M, ctx->mat, ctx->M, ctx->N);
+    k_state_in<float><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(M, material, ctx->mat, ctx->M, ctx->N,
+                                                                    ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
-    k_set_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate, t, t, 0.0);
-    MMS_LAUNCH_CHECK(ctx);
-    MMS_TRY(clear_numeric_flag(ctx));
     ctx->state_ready = true;
     ctx->phi_valid = false;
     return MMS_OK;
@@ -732,11 +717,9 @@ int mms_state_set_f32(mms_ctx *ctx, const uint8_t *material, const float *M, dou
     float *stage = reinterpret_cast<float *>(ctx->K);
     MMS_CUDA_TRY(cudaMemcpyAsync(ctx->mat, material, n, cudaMemcpyHostToDevice, ctx->stream));
     MMS_CUDA_TRY(cudaMemcpyAsync(stage, M, 3 * n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-    k_aos32_to_soa<<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(stage, ctx->mat, ctx->M, ctx->N);
+    k_state_in<float><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(stage, ctx->mat, ctx->mat, ctx->M, ctx->N,
+                                                                    ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
-    k_set_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate, t, t, 0.0);
-    MMS_LAUNCH_CHECK(ctx);
-    MMS_TRY(clear_numeric_flag(ctx));
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     ctx->state_ready = true;
     ctx->phi_valid = false;
