@@ -195,7 +195,6 @@ int rk4_step_kernels(mms_ctx *ctx, bool eval_first)
     MMS_TRY(eval_state_potential(ctx, ctx->A));
     MMS_TRY(launch_rk4_stage(ctx, 3, ctx->A, nullptr));
     if (!eval_first) MMS_TRY(eval_state_potential(ctx, ctx->M));
-    MMS_TRY(launch_advance_time(ctx));
     return MMS_OK;
 }
 
@@ -618,6 +617,7 @@ int mms_state_set_dev(mms_ctx *ctx, const uint8_t *material, const double *M, do
     k_state_in<double><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(M, material, ctx->mat, ctx->M, ctx->N,
                                                                      ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
+    ctx->dt_known = false;
     ctx->state_ready = true;
     ctx->phi_valid = false;
     return MMS_OK;
@@ -635,6 +635,7 @@ int mms_state_set(mms_ctx *ctx, const uint8_t *material, const double *M, double
     k_state_in<double><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->K, ctx->mat, ctx->mat, ctx->M, ctx->N,
                                                                      ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
+    ctx->dt_known = false;
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     ctx->state_ready = true;
     ctx->phi_valid = false;
@@ -687,6 +688,7 @@ int mms_state_set_f32_dev(mms_ctx *ctx, const uint8_t *material, const float *M,
     k_state_in<float><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(M, material, ctx->mat, ctx->M, ctx->N,
                                                                     ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
+    ctx->dt_known = false;
     ctx->state_ready = true;
     ctx->phi_valid = false;
     return MMS_OK;
@@ -720,6 +722,7 @@ int mms_state_set_f32(mms_ctx *ctx, const uint8_t *material, const float *M, dou
     k_state_in<float><<<div_up(ctx->N, 256), 256, 0, ctx->stream>>>(stage, ctx->mat, ctx->mat, ctx->M, ctx->N,
                                                                     ctx->tstate, ctx->stats, t);
     MMS_LAUNCH_CHECK(ctx);
+    ctx->dt_known = false;
     MMS_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     ctx->state_ready = true;
     ctx->phi_valid = false;
@@ -756,8 +759,14 @@ int mms_run_fixed(mms_ctx *ctx, double dt, int nsteps, int use_graph)
         mms_set_error("dt must be positive and nsteps >= 0");
         return MMS_ERR_ARG;
     }
-    k_set_dt<<<1, 1, 0, ctx->stream>>>(ctx->tstate, dt);
-    MMS_LAUNCH_CHECK(ctx);
+    // the device keeps dt between calls: a caller stepping with one dt
+    // launches the step graph alone
+    if (!ctx->dt_known || ctx->dt_dev != dt) {
+        k_set_dt<<<1, 1, 0, ctx->stream>>>(ctx->tstate, dt);
+        MMS_LAUNCH_CHECK(ctx);
+        ctx->dt_known = true;
+        ctx->dt_dev = dt;
+    }
     int left = nsteps;
     while (left > 0 && surrogate_armed(ctx)) {
         const int chunk = (int)std::min<long long>(left, ctx->sur_every - ctx->sur_since);
@@ -829,6 +838,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
                                      ctx->stream));
         k_set_time<<<1, 1, 0, ctx->stream>>>(ctx->tstate, t_, tk1_, 0.0);
         MMS_LAUNCH_CHECK(ctx);
+        ctx->dt_known = false;
         ctx->phi_valid = true;
         return MMS_OK;
     };
@@ -868,6 +878,7 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
             MMS_TRY(backup());
             k_set_dt<<<1, 1, 0, ctx->stream>>>(ctx->tstate, dt);
             MMS_LAUNCH_CHECK(ctx);
+            ctx->dt_known = false;
             MMS_TRY(run_steps(ctx, 1, 0));
             MMS_TRY(launch_stats(ctx));
             MMS_TRY(read_stats(ctx, st));
@@ -913,12 +924,14 @@ int mms_march(mms_ctx *ctx, const mms_controller *ctl, double finaltime, double 
             MMS_TRY(backup());
             k_set_dt<<<1, 1, 0, ctx->stream>>>(ctx->tstate, h);
             MMS_LAUNCH_CHECK(ctx);
+            ctx->dt_known = false;
             MMS_TRY(run_steps(ctx, 1, 0));
             MMS_CUDA_TRY(cudaMemcpyAsync(ctx->Mfull, ctx->M, n3 * sizeof(double), cudaMemcpyDeviceToDevice,
                                          ctx->stream));
             MMS_TRY(restore(t, tk1));
             k_set_dt<<<1, 1, 0, ctx->stream>>>(ctx->tstate, 0.5 * h);
             MMS_LAUNCH_CHECK(ctx);
+            ctx->dt_known = false;
             MMS_TRY(run_steps(ctx, 2, 0));
             const unsigned nb = div_up(ctx->N, 256);
             k_maxdiff_part<<<nb, 256, 0, ctx->stream>>>(ctx->Mfull, ctx->M, ctx->mat, ctx->stat_part, ctx->N);

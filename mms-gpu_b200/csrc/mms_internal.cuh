@@ -93,6 +93,9 @@ inline void physk_derive(PhysK &k, double dx, double dy, double dz)
 //   [2] t_k1   time at which H(M) (the k1 field) was evaluated; equals t
 //              except in reference-stage-time mode (see mms_params)
 constexpr int TIME_T = 0, TIME_DT = 1, TIME_TK1 = 2, TIME_SLOTS = 4;
+//   [3] (low 32 bits) arrival counter of the last RK4 stage's CTAs: the last
+//       to finish advances the time and resets it (k_rk4_stage)
+constexpr int TIME_CTR = 3;
 
 // statistics block: sums over material cells, finished on device
 //   [0] sum M.H  [1] max |MxH|  [2..4] sum M  [5] sum |M|  [6] count  [7] nonfinite flag
@@ -140,6 +143,8 @@ struct mms_ctx {
 
     bool state_ready = false;
     bool phi_valid = false;                     // phi holds the potential of M
+    bool dt_known = false;                      // tstate's dt is dt_dev (set by mms_run_fixed)
+    double dt_dev = 0.0;
 
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -163,8 +168,8 @@ int launch_divergence_aos(mms_ctx *ctx, const float *M, float *rho);
 int launch_gradient_aos(mms_ctx *ctx, const float *phi, double c, float *H);
 int launch_exchange_aos(mms_ctx *ctx, const float *M, float *H);
 int launch_hfield_aos(mms_ctx *ctx, const float *M, const float *phi, double t, float *H);
+// stage 3 also advances the state's time (t_k1 = t, t += dt)
 int launch_rk4_stage(mms_ctx *ctx, int stage, const double *Mst, double *Mnext);
-int launch_advance_time(mms_ctx *ctx);
 int launch_stats(mms_ctx *ctx);
 
 int direct_build_table(mms_ctx *ctx);

@@ -171,15 +171,13 @@ __global__ void k_div_soa(const double *__restrict__ M, float *__restrict__ rho,
 //   stage 2: K += 2 k3;     Mnext = M + dt   k3
 //   stage 3: K += k4;       M = renorm(M + dt/6 K) (Mnext unused, written in place)
 // Empty cells keep M = 0 in every buffer.
-__global__ void __launch_bounds__(TPB) k_rk4_stage(const float *__restrict__ phi, const double *__restrict__ Mst,
-                                                   double *__restrict__ M, double *__restrict__ K,
-                                                   double *__restrict__ Mnext, const uint8_t *__restrict__ mat,
-                                                   const double *__restrict__ tstate, const double *__restrict__ htab,
-                                                   double *__restrict__ stats, GridK g, PhysK p, int stage)
+__device__ __forceinline__ void rk4_stage_cell(long long i, const float *__restrict__ phi,
+                                               const double *__restrict__ Mst, double *__restrict__ M,
+                                               double *__restrict__ K, double *__restrict__ Mnext,
+                                               const uint8_t *__restrict__ mat, const double *__restrict__ tstate,
+                                               const double *__restrict__ htab, double *__restrict__ stats,
+                                               const GridK &g, const PhysK &p, int stage)
 {
-    pdl_begin();
-    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= g.N) return;
     const long long N = g.N;
     const double t = tstate[TIME_T], dt = tstate[TIME_DT];
     if (!mat[i]) {
@@ -239,13 +237,34 @@ __global__ void __launch_bounds__(TPB) k_rk4_stage(const float *__restrict__ phi
     }
 }
 
-__global__ void k_advance_time(double *tstate)
+
+// The stage kernel: thread per cell.  At the last stage (advance != 0) the
+// last CTA to finish also advances the time of the state, so that no launch
+// of its own follows the step: every CTA has read t and dt before it arrives
+// on the counter, and the counter is reset for the next step.
+__global__ void __launch_bounds__(TPB) k_rk4_stage(const float *__restrict__ phi, const double *__restrict__ Mst,
+                                                   double *__restrict__ M, double *__restrict__ K,
+                                                   double *__restrict__ Mnext, const uint8_t *__restrict__ mat,
+                                                   double *__restrict__ tstate, const double *__restrict__ htab,
+                                                   double *__restrict__ stats, GridK g, PhysK p, int stage,
+                                                   int advance)
 {
     pdl_begin();
-    // t_k1: time at which the next step's k1 field is taken.  The reference
-    // evaluates the post-step field at the OLD t (ode_functions.cpp:267).
-    tstate[TIME_TK1] = tstate[TIME_T];
-    tstate[TIME_T] += tstate[TIME_DT];
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < g.N) rk4_stage_cell(i, phi, Mst, M, K, Mnext, mat, tstate, htab, stats, g, p, stage);
+    if (!advance) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned *ctr = reinterpret_cast<unsigned *>(tstate + TIME_CTR);
+        if (atomicAdd(ctr, 1u) == gridDim.x - 1) {
+            // t_k1: the time at which the next step's k1 field is taken (the
+            // reference evaluates the post-step field at the OLD t,
+            // ode_functions.cpp:267)
+            tstate[TIME_TK1] = tstate[TIME_T];
+            tstate[TIME_T] += tstate[TIME_DT];
+            *ctr = 0u;
+        }
+    }
 }
 
 __device__ __forceinline__ double warp_sum(double v)
@@ -431,15 +450,8 @@ int launch_rk4_stage(mms_ctx *ctx, int stage, const double *Mst, double *Mnext)
 {
     MMS_CUDA_TRY(launch_k(k_rk4_stage, dim3(div_up(ctx->N, TPB)), dim3(TPB), 0, ctx->stream,
                           (const float *)ctx->phi, Mst, ctx->M, ctx->K, Mnext, (const uint8_t *)ctx->mat,
-                          (const double *)ctx->tstate, (const double *)ctx->hext, ctx->stats, ctx->gk(),
-                          ctx->pk(), stage));
-    MMS_LAUNCH_CHECK(ctx);
-    return MMS_OK;
-}
-
-int launch_advance_time(mms_ctx *ctx)
-{
-    MMS_CUDA_TRY(launch_k(k_advance_time, dim3(1), dim3(1), 0, ctx->stream, ctx->tstate));
+                          ctx->tstate, (const double *)ctx->hext, ctx->stats, ctx->gk(), ctx->pk(), stage,
+                          stage == 3 ? 1 : 0));
     MMS_LAUNCH_CHECK(ctx);
     return MMS_OK;
 }
