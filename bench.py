@@ -95,20 +95,7 @@ class ClockSampler:
         self.smax = None
         self.run = False
         try:
-            import pynvml
-            pynvml.nvmlInit()
-            h = None
-            try:
-                import torch
-                bus = getattr(torch.cuda.get_device_properties(device_index), "pci_bus_id", None)
-                dom = getattr(torch.cuda.get_device_properties(device_index), "pci_domain_id", 0)
-                dev = getattr(torch.cuda.get_device_properties(device_index), "pci_device_id", 0)
-                if bus is not None:
-                    h = pynvml.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dev:02x}.0")
-            except Exception:
-                h = None
-            if h is None:
-                h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            pynvml, h = nvml_handle(device_index)
             self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
             self.bits = (pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
                          pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap)
@@ -402,6 +389,14 @@ def run_ours(args):
     # same loop with the FP64 state calls is reported beside it.
     e2e = None
     if not args.no_e2e:
+        # pinned host buffers on the GPU's NUMA node: the process runs on the
+        # GPU's local CPUs while they are allocated (first touch places the
+        # pages), as a serving process would be bound; host copies from a
+        # remote node measured 12 GB/s H2D against 48 from a local one
+        affinity0 = os.sched_getaffinity(0)
+        local = gpu_local_cpus(torch.cuda.current_device())
+        if local:
+            os.sched_setaffinity(0, local)
         M64 = ctx.state_get()[0]
         host_mat = torch.from_numpy(mask.astype(np.uint8)).pin_memory()
         dev_mat = torch.empty(host_mat.shape, dtype=torch.uint8, device="cuda")
@@ -481,6 +476,9 @@ def run_ours(args):
                        "frac_of_bound": e2e["value"] / bound,
                        "note": "bound = 1 / (device step time + H2D bytes / H2D bandwidth + D2H bytes / D2H "
                                "bandwidth): the copies and the step are serial in a round trip"}
+        e2e["host_buffers"] = (f"pinned while the process ran on the {len(local)} CPUs local to the GPU (NVML)"
+                               if local else "pinned; GPU-local CPUs unknown, process not bound")
+        os.sched_setaffinity(0, affinity0)
 
     sur = None
     if args.solver == "fmm" and not args.no_surrogate:
@@ -640,6 +638,39 @@ def surrogate_block(args, grid, params, mask, M, stream, flush, fmm_value):
         matched.append(row)
     out["fmm_at_matched_accuracy"] = matched
     return out
+
+
+def nvml_handle(device_index):
+    """(pynvml, handle) of the torch device, found by PCI bus id; raises
+    when NVML is not there"""
+    import pynvml
+    pynvml.nvmlInit()
+    h = None
+    try:
+        import torch
+        props = torch.cuda.get_device_properties(device_index)
+        bus = getattr(props, "pci_bus_id", None)
+        if bus is not None:
+            dom, dev = getattr(props, "pci_domain_id", 0), getattr(props, "pci_device_id", 0)
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(f"{dom:08x}:{bus:02x}:{dev:02x}.0")
+    except Exception:
+        h = None
+    if h is None:
+        h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+    return pynvml, h
+
+
+def gpu_local_cpus(device_index):
+    """the CPUs NVML lists as local to the GPU (its NUMA node), within this
+    process's current affinity; None when unknown"""
+    try:
+        pynvml, h = nvml_handle(device_index)
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
+        cpus = {64 * w + b for w, word in enumerate(words) for b in range(64) if (word >> b) & 1}
+        cpus &= os.sched_getaffinity(0)
+        return cpus or None
+    except Exception:
+        return None
 
 
 def pcie_bandwidth(stream, nbytes=32 << 20, reps=5):
