@@ -389,14 +389,6 @@ def run_ours(args):
     # same loop with the FP64 state calls is reported beside it.
     e2e = None
     if not args.no_e2e:
-        # pinned host buffers on the GPU's NUMA node: the process runs on the
-        # GPU's local CPUs while they are allocated (first touch places the
-        # pages), as a serving process would be bound; host copies from a
-        # remote node measured 12 GB/s H2D against 48 from a local one
-        affinity0 = os.sched_getaffinity(0)
-        local = gpu_local_cpus(torch.cuda.current_device())
-        if local:
-            os.sched_setaffinity(0, local)
         M64 = ctx.state_get()[0]
         host_mat = torch.from_numpy(mask.astype(np.uint8)).pin_memory()
         dev_mat = torch.empty(host_mat.shape, dtype=torch.uint8, device="cuda")
@@ -476,9 +468,6 @@ def run_ours(args):
                        "frac_of_bound": e2e["value"] / bound,
                        "note": "bound = 1 / (device step time + H2D bytes / H2D bandwidth + D2H bytes / D2H "
                                "bandwidth): the copies and the step are serial in a round trip"}
-        e2e["host_buffers"] = (f"pinned while the process ran on the {len(local)} CPUs local to the GPU (NVML)"
-                               if local else "pinned; GPU-local CPUs unknown, process not bound")
-        os.sched_setaffinity(0, affinity0)
 
     sur = None
     if args.solver == "fmm" and not args.no_surrogate:
@@ -658,19 +647,6 @@ def nvml_handle(device_index):
     if h is None:
         h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
     return pynvml, h
-
-
-def gpu_local_cpus(device_index):
-    """the CPUs NVML lists as local to the GPU (its NUMA node), within this
-    process's current affinity; None when unknown"""
-    try:
-        pynvml, h = nvml_handle(device_index)
-        words = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
-        cpus = {64 * w + b for w, word in enumerate(words) for b in range(64) if (word >> b) & 1}
-        cpus &= os.sched_getaffinity(0)
-        return cpus or None
-    except Exception:
-        return None
 
 
 def pcie_bandwidth(stream, nbytes=32 << 20, reps=5):
