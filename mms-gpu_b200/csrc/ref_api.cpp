@@ -8,6 +8,12 @@
 #include <string.h>
 #include <sys/stat.h>
 
+#include <algorithm>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "mms_b200.h"
@@ -180,24 +186,132 @@ int rk4_step(const fptype t, const fptype dt, fptype *t2, const byte *material, 
 
 namespace {
 
+// Mdynamics.dat: one snapshot of M per accepted step in the layout of
+// helper_functions.cpp:107-123 (per z, x outer, y inner, "%g %g %g \n").
+// Formatting a snapshot of a large grid takes far longer than the GPU step,
+// so snapshots are formatted on worker threads (the (z, x) columns split into
+// chunks that are written in order) by a writer thread while marching goes
+// on.  At most kDepth snapshots wait; the caller then blocks until one is
+// written, so every snapshot is written, in order, and memory stays bounded.
+class SnapshotWriter {
+public:
+    static constexpr int kDepth = 3;
+
+    SnapshotWriter(FILE *fh, int zdim, int ydim, int xdim) : fh_(fh), Z_(zdim), Y_(ydim), X_(xdim)
+    {
+        const unsigned hc = std::thread::hardware_concurrency();
+        nthreads_ = (int)std::max(1u, std::min(8u, hc ? hc : 1u));
+        bufs_.resize(kDepth);
+        for (auto &b : bufs_) {
+            b.resize(3 * (size_t)zdim * ydim * xdim);
+            free_.push_back(b.data());
+        }
+        th_ = std::thread([this] { run(); });
+    }
+    ~SnapshotWriter() { finish(); }
+
+    // a buffer of 3 N floats to fill (blocks while every buffer waits)
+    float *acquire()
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [this] { return !free_.empty(); });
+        float *b = free_.front();
+        free_.pop_front();
+        return b;
+    }
+    // queue a filled buffer; release an unfilled one
+    void submit(float *b)
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            queue_.push_back(b);
+        }
+        cv_.notify_all();
+    }
+    void release(float *b)
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            free_.push_back(b);
+        }
+        cv_.notify_all();
+    }
+    // write everything queued and stop; false if a write failed
+    bool finish()
+    {
+        if (th_.joinable()) {
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                stop_ = true;
+            }
+            cv_.notify_all();
+            th_.join();
+        }
+        return ok_;
+    }
+
+private:
+    void run()
+    {
+        for (;;) {
+            float *b;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [this] { return stop_ || !queue_.empty(); });
+                if (queue_.empty()) return;  // stop_ and nothing left
+                b = queue_.front();
+                queue_.pop_front();
+            }
+            write(b);
+            release(b);
+        }
+    }
+
+    void format(const float *m, long long o0, long long o1, std::string &out) const
+    {
+        char line[96];
+        for (long long o = o0; o < o1; o++) {
+            const int z = (int)(o / X_), x = (int)(o % X_);
+            for (int y = 0; y < Y_; y++) {
+                const size_t i = (size_t)z * Y_ * X_ + (size_t)y * X_ + x;
+                const int n = snprintf(line, sizeof line, "%g %g %g \n", m[3 * i], m[3 * i + 1], m[3 * i + 2]);
+                out.append(line, (size_t)n);
+            }
+        }
+    }
+
+    void write(const float *m)
+    {
+        const long long cols = (long long)Z_ * X_;
+        const int T = (int)std::min<long long>(nthreads_, std::max<long long>(1, cols));
+        std::vector<std::string> parts(T);
+        std::vector<std::thread> workers;
+        for (int k = 1; k < T; k++)
+            workers.emplace_back([this, m, cols, T, k, &parts] { format(m, cols * k / T, cols * (k + 1) / T, parts[k]); });
+        format(m, 0, cols / T, parts[0]);
+        for (auto &w : workers) w.join();
+        for (const auto &p : parts)
+            if (!p.empty() && fwrite(p.data(), 1, p.size(), fh_) != p.size()) ok_ = false;
+    }
+
+    FILE *fh_;
+    int Z_, Y_, X_;
+    int nthreads_ = 1;
+    std::vector<std::vector<float>> bufs_;
+    std::deque<float *> free_, queue_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    bool stop_ = false;
+    bool ok_ = true;  // written only by the writer thread, read after join
+    std::thread th_;
+};
+
 struct MarchLog {
     mms_ctx *ctx;
     FILE *fh, *fhM, *fhp;
-    int xdim, ydim, zdim;
-    std::vector<float> m;  // the state in the reference's FP32 Vector3 layout
+    SnapshotWriter *snap;
     int status;
 };
-
-// helper_functions.cpp:107-123 layout: per z, x outer, y inner, "%g %g %g \n"
-void append_vector3d(FILE *fh, const float *m, int zdim, int ydim, int xdim)
-{
-    for (int z = 0; z < zdim; z++)
-        for (int x = 0; x < xdim; x++)
-            for (int y = 0; y < ydim; y++) {
-                const size_t i = (size_t)z * ydim * xdim + (size_t)y * xdim + x;
-                fprintf(fh, "%g %g %g \n", m[3 * i], m[3 * i + 1], m[3 * i + 2]);
-            }
-}
 
 int march_cb(void *user, int rejected, const mms_record *r)
 {
@@ -210,11 +324,13 @@ int march_cb(void *user, int rejected, const mms_record *r)
         return 0;
     }
     double t;
-    if (mms_state_get_f32(L->ctx, L->m.data(), &t) != MMS_OK) {
+    float *buf = L->snap->acquire();
+    if (mms_state_get_f32(L->ctx, buf, &t) != MMS_OK) {
+        L->snap->release(buf);
         L->status = EXIT_FAILURE;
         return 1;
     }
-    append_vector3d(L->fhM, L->m.data(), L->zdim, L->ydim, L->xdim);
+    L->snap->submit(buf);
     // ode_functions.cpp:330-333
     fprintf(L->fh, "%d, %g, %g, %g, %g, %g, %g, %g, %g \n", r->tindex, (fptype)r->t, (fptype)r->dt, (fptype)r->E_eV,
             (fptype)r->Mx, (fptype)r->My, (fptype)r->Mz, (fptype)r->Mmag, (fptype)r->torque);
@@ -239,9 +355,7 @@ int time_marching(byte *material, Vector3 *M, const fptype finaltime, const fpty
     char fn[1100];
     MarchLog L;
     L.ctx = ctx;
-    L.xdim = xdim;
-    L.ydim = ydim;
-    L.zdim = zdim;
+    L.snap = nullptr;
     L.status = EXIT_SUCCESS;
     snprintf(fn, sizeof fn, "%s/%s", sim_name, "dynamics.dat");
     L.fh = fopen(fn, "w");
@@ -256,8 +370,8 @@ int time_marching(byte *material, Vector3 *M, const fptype finaltime, const fpty
         if (L.fhp) fclose(L.fhp);
         return EXIT_FAILURE;
     }
-    const size_t n = (size_t)xdim * ydim * zdim;
-    L.m.resize(3 * n);
+    SnapshotWriter snap(L.fhM, zdim, ydim, xdim);
+    L.snap = &snap;
     int st = mms_state_set_f32(ctx, material, &M[0].x, 0.0);
     if (st == MMS_OK) {
         mms_controller c;
@@ -277,6 +391,10 @@ int time_marching(byte *material, Vector3 *M, const fptype finaltime, const fpty
     if (st == MMS_OK) {
         double t;
         st = mms_state_get_f32(ctx, &M[0].x, &t);
+    }
+    if (!snap.finish()) {
+        printf("FATAL ERROR: writing Mdynamics.dat in %s failed\n", sim_name);
+        L.status = EXIT_FAILURE;
     }
     fclose(L.fh);
     fclose(L.fhM);

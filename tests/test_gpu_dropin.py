@@ -32,6 +32,19 @@ def read_dynamics(path):
     return np.array(rows)
 
 
+def read_snapshots(path, ncell=16 * 16 * 3):
+    """Mdynamics.dat as [snapshot][line][3]: lines of exactly three numbers"""
+    vals = []
+    with open(path) as f:
+        for line in f:
+            parts = line.split()
+            assert len(parts) == 3, line
+            vals.append([float(v) for v in parts])
+    a = np.array(vals)
+    assert len(a) % ncell == 0
+    return a.reshape(-1, ncell, 3)
+
+
 @pytest.mark.parametrize("run", ["sd", "vortex_ext"])
 def test_reference_main_runs_on_the_gpu(cuda, lib, run):
     if not os.path.exists(DROPIN):
@@ -44,7 +57,13 @@ def test_reference_main_runs_on_the_gpu(cuda, lib, run):
                            timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         rows = read_dynamics(os.path.join(td, args[15], "dynamics.dat"))
-        assert os.path.getsize(os.path.join(td, args[15], "Mdynamics.dat")) > 0
+        snaps = read_snapshots(os.path.join(td, args[15], "Mdynamics.dat"))
+    # one snapshot of the 16 x 16 x 3 cells per accepted step, every one
+    # written (the writer thread formats them while marching goes on), each
+    # cell |M| = Ms or empty
+    assert snaps.shape == (len(rows), 16 * 16 * 3, 3)
+    mag = np.linalg.norm(snaps, axis=-1)
+    assert np.all((np.abs(mag - 8.6e5) < 8.6e5 * 1e-5) | (mag == 0))
     n = min(100, len(rows), len(ref_rows))
     assert n >= 50
     assert np.array_equal(rows[:n, 0], ref_rows[:n, 0])
