@@ -191,3 +191,34 @@ def test_fp32_vector3_state_io(cuda, lib):
     assert np.array_equal(Mb32, Ma.astype(np.float32))
     assert np.array_equal(Mc32, Mb32)
     assert np.all(Mb32[mat == 0] == 0) and np.all(Ma[mat == 0] == 0)
+
+
+def test_time_and_dt_across_calls(cuda, lib):
+    """the last stage advances the time; mms_run_fixed sets dt on the device
+    only when it changes, and a state set (which clears dt) makes the next
+    call set it again: t follows every call's dt, and the same steps taken
+    with a change of dt between them match a context stepping them in one
+    go where the dt is the same"""
+    import mmsb200
+    z = golden("rk4_16x16x3.npz")
+    dims, d = dims_of(z)
+    g = mmsb200.Grid(*dims, *d)
+    mat, M0 = z["material"], z["M0"].astype(np.float64)
+    d1, d2 = 1e-13, 2.5e-14
+    with mmsb200.Context(g, mmsb200.make_params(external=True)) as a, \
+            mmsb200.Context(g, mmsb200.make_params(external=True)) as b:
+        a.state_set(mat, M0)
+        a.run_fixed(d1, 2)
+        a.run_fixed(d2, 1)
+        a.run_fixed(d1, 1)
+        Ma, ta = a.state_get()
+        assert abs(ta - (3 * d1 + d2)) < 1e-26
+        a.state_set(mat, M0, 1e-12)
+        a.run_fixed(d1, 1)  # same dt as the last call: set again after the state set
+        assert abs(a.state_get()[1] - (1e-12 + d1)) < 1e-26
+        b.state_set(mat, M0)
+        b.run_fixed(d1, 2, use_graph=False)
+        b.run_fixed(d2, 1, use_graph=False)
+        b.run_fixed(d1, 1, use_graph=False)
+        Mb, tb = b.state_get()
+    assert ta == tb and np.array_equal(Ma, Mb)
